@@ -1,0 +1,103 @@
+"""CPU oracle for the trace misfits and their adjoint sources.
+
+TEST INFRASTRUCTURE ONLY: the parity tests, smoke() and bench.py's
+cpu_baseline / reference legs use it as the checker; the product path never
+imports it.
+
+Restates the reference's ``adjoint_functions.py`` (Otfwi project root):
+  * ``L2``          adjoint_functions.py:8-11
+  * ``wasserstein`` adjoint_functions.py:25-67 (the misfit regression.py:42 uses)
+
+The reference computes through two scipy routines that are not part of the
+reference tree (scipy 1.18.1 is the version installed beside it). Their
+published algorithms are restated here so the same arithmetic can be mirrored
+on the GPU:
+  * ``scipy.integrate.cumulative_trapezoid(y, x, initial=0)``:
+        res = cumsum(diff(x) * (y[1:] + y[:-1]) / 2.0), prefixed by 0;
+        with no x the spacing is the scalar 1.0;
+  * ``scipy.interpolate.interp1d(x, y, kind='linear',
+        fill_value='extrapolate')``: x is stably sorted (mergesort argsort);
+        an evaluation point xn takes i = searchsorted(x, xn, 'left') clipped to
+        [1, n-1], lo = i-1, hi = i, and returns
+        ((xn - x_lo)/(x_hi - x_lo))*y_hi + ((x_hi - xn)/(x_hi - x_lo))*y_lo,
+        extrapolating with the first / last segment.
+The operations and their order are the reference's, so on the same inputs
+this oracle reproduces the reference bit for bit (pinned by
+tests/golden/misfit_*.npz, generated from the reference itself).
+"""
+import numpy as np
+
+
+def cumtrapz0(y, x=None):
+    """cumulative_trapezoid(y, x, initial=0) in float64."""
+    y = np.asarray(y, dtype=np.float64)
+    d = np.diff(np.asarray(x, dtype=np.float64)) if x is not None else 1.0
+    res = np.cumsum(d * (y[1:] + y[:-1]) / 2.0)
+    return np.concatenate((np.zeros(1, dtype=res.dtype), res))
+
+
+class Interp1dLinear:
+    """interp1d(x, y, kind='linear', fill_value='extrapolate', assume_sorted=False)."""
+
+    def __init__(self, x, y):
+        x = np.array(x, dtype=np.float64)
+        y = np.array(y, dtype=np.float64)
+        ind = np.argsort(x, kind="mergesort")
+        self.x = x[ind]
+        self.y = y[ind]
+
+    def __call__(self, xn):
+        xn = np.asarray(xn, dtype=np.float64)
+        idx = np.searchsorted(self.x, xn).clip(1, len(self.x) - 1).astype(int)
+        lo = idx - 1
+        hi = idx
+        x_lo = self.x[lo]
+        x_hi = self.x[hi]
+        y_lo = self.y[lo]
+        y_hi = self.y[hi]
+        return ((xn - x_lo) / (x_hi - x_lo)) * y_hi + ((x_hi - xn) / (x_hi - x_lo)) * y_lo
+
+
+def L2(sim, obs):
+    """adjoint_functions.py:8-11: J = sum (sim-obs)^2, adjoint = sim - obs."""
+    resid = np.asarray(sim, dtype=np.float64) - obs
+    mse = np.sum(resid ** 2)
+    return mse, resid
+
+
+def wasserstein_trace(sim_s, obs_s, t, dt):
+    """One trace of adjoint_functions.py:33-64; returns (W2 term, adjoint row)."""
+    f_gate = np.concatenate([np.zeros(0), np.asarray(sim_s)])
+    g_gate = np.concatenate([np.zeros(0), np.asarray(obs_s)])
+    c = -1.1 * np.min(g_gate)
+    c = np.maximum(c, 0.1 * np.max(g_gate))
+    g = g_gate + c
+    f = f_gate + c
+    g /= np.sum(g * dt)
+    f /= np.sum(f * dt)
+    G = cumtrapz0(g, t)
+    F = cumtrapz0(f, t)
+    F_i = Interp1dLinear(t, F)
+    F_1 = Interp1dLinear(F, t)
+    G_1 = Interp1dLinear(G, t)
+    dist = Interp1dLinear(t, 2 * cumtrapz0(t - G_1(F_i(t))))
+    adj = dist(t) - dist(1)
+    w2 = sum(np.abs(F_1(t) - G_1(t)) ** 2)
+    return w2, adj
+
+
+def wasserstein(sim, obs):
+    """adjoint_functions.py:25-67: per-trace quadratic Wasserstein misfit of
+    shifted, rectangle-normalised traces and its adjoint source."""
+    sim = np.asarray(sim)
+    obs = np.asarray(obs)
+    n_sens, T = sim.shape
+    t = np.linspace(0, 1, T)
+    dt = t[1] - t[0]
+    W2 = 0
+    s_W2 = np.zeros((n_sens, T))
+    for s in range(n_sens):
+        w2, adj = wasserstein_trace(sim[s], obs[s], t, dt)
+        s_W2[s, :] = adj
+        W2 += w2
+    return W2, s_W2

@@ -1,0 +1,776 @@
+// Engine implementation: device buffers, per-tile point tables, CUDA graphs
+// of the time loops, and the small helper kernels around the fused steps.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "engine.h"
+
+namespace otf {
+
+const TileShape kTileShapes[kNumTileShapes] = {{56, 56}, {120, 24}, {120, 56}, {248, 24}};
+
+// ---------------------------------------------------------------- errors
+static thread_local int g_status = 0;
+static thread_local std::string g_msg;
+
+void set_error(int code, const char *what, const char *file, int line)
+{
+    g_status = code ? code : -1;
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what,
+             cudaGetErrorString((cudaError_t)code), file, line);
+    g_msg = buf;
+}
+void set_error_msg(int code, const std::string &msg)
+{
+    g_status = code ? code : -1;
+    g_msg = msg;
+}
+void clear_error()
+{
+    g_status = 0;
+    g_msg.clear();
+}
+int last_status() { return g_status; }
+const char *last_error() { return g_msg.c_str(); }
+
+// ---------------------------------------------------------- helper kernels
+
+// Running integral of each row (somaFonteIntegral's "integral[n] +=",
+// regression_PML_single.cu:285-288): tab[r][t] = sum_{u=1..t} s[r][u], or of
+// the time-flipped series s[r][T-1-u]; sequential FP32 adds in the
+// reference's order, tab[r][0] = 0.
+__global__ void k_prefix_rows(const float *__restrict__ src, float *__restrict__ tab, int rows,
+                              int T, int flip)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows)
+        return;
+    const float *s = src + (int64_t)r * T;
+    float *o = tab + (int64_t)r * T;
+    float acc = 0.f;
+    o[0] = 0.f;
+    for (int t = 1; t < T; t++) {
+        acc = __fadd_rn(acc, flip ? s[T - 1 - t] : s[t]);
+        o[t] = acc;
+    }
+}
+
+// Padded P coefficients from c^2: forward / adjoint (c2*dt)/dx
+// (regression_PML_single.cu:512) and reconstruction c2*(dt/dx) (:517).
+__global__ void k_prep_q(const float *__restrict__ cq, float *__restrict__ qf,
+                         float *__restrict__ qr, Layout L, float dx, float dt)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.slot)
+        return;
+    const int prow = (int)(i / L.pitch), pcol = (int)(i - (int64_t)prow * L.pitch);
+    const int x = pcol - PAD, z = prow - PAD;
+    float vf = 0.f, vr = 0.f;
+    if (x >= 0 && x < L.X && z >= 0 && z < L.Z) {
+        const float c = cq[(int64_t)z * L.X + x];
+        vf = __fdiv_rn(__fmul_rn(c, dt), dx);
+        vr = __fmul_rn(c, __fdiv_rn(dt, dx));
+    }
+    qf[i] = vf;
+    if (qr)
+        qr[i] = vr;
+}
+
+// Sum of the padded per-shot gradients into an unpadded [Z*X] array, in shot
+// order (the wrapper's grad_acc += grad loop, cuda_interface_pml.py:225-235),
+// then scaled.
+__global__ void k_grad_sum(const float *__restrict__ g, float *__restrict__ out, Layout L,
+                           int n_shots, int64_t stride, float scale)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)L.X * L.Z)
+        return;
+    const int z = (int)(i / L.X), x = (int)(i - (int64_t)z * L.X);
+    const int64_t o = L.at(x, z);
+    float acc = 0.f;
+    for (int s = 0; s < n_shots; s++)
+        acc = __fadd_rn(acc, g[o + stride * s]);
+    out[i] = scale == 1.f ? acc : __fmul_rn(acc, scale);
+}
+
+// ------------------------------------------------------- kernel dispatch
+
+struct KernelSet {
+    void (*fwd)(const StepParams);
+    void (*fwd_ring)(const StepParams);
+    void (*rev)(const StepParams);
+    size_t smem;
+};
+
+template <int TX, int TZ, class Prec, bool SEP>
+static KernelSet make_set()
+{
+    KernelSet k;
+    k.fwd = k_forward_step<TX, TZ, Prec, SEP, false>;
+    k.fwd_ring = k_forward_step<TX, TZ, Prec, SEP, true>;
+    k.rev = k_reverse_step<TX, TZ, Prec, SEP>;
+    k.smem = (size_t)TileGeom<TX, TZ>::SMEM_FLOATS * sizeof(float);
+    return k;
+}
+
+template <int TX, int TZ>
+static void fill_shape(KernelSet (&s)[2][2])
+{
+    s[kFaithful][1] = make_set<TX, TZ, Faithful, true>();
+    s[kFast][1] = make_set<TX, TZ, Fast, true>();
+    s[kFaithful][0] = KernelSet{nullptr, nullptr, nullptr, 0};
+    s[kFast][0] = KernelSet{nullptr, nullptr, nullptr, 0};
+}
+
+struct KernelTable {
+    KernelSet s[kNumTileShapes][2][2];  // [shape][precision][separable]
+    bool attrs_set = false;
+    KernelTable()
+    {
+        fill_shape<56, 56>(s[0]);
+        fill_shape<120, 24>(s[1]);
+        fill_shape<120, 56>(s[2]);
+        fill_shape<248, 24>(s[3]);
+        // general (non-separable) damping: compiled for the first shape only
+        s[0][kFaithful][0] = make_set<56, 56, Faithful, false>();
+        s[0][kFast][0] = make_set<56, 56, Fast, false>();
+    }
+    int set_attrs()
+    {
+        if (attrs_set)
+            return 0;
+        for (auto &a : s)
+            for (auto &b : a)
+                for (auto &k : b) {
+                    if (!k.fwd)
+                        continue;
+                    void (*fns[3])(const StepParams) = {k.fwd, k.fwd_ring, k.rev};
+                    for (auto f : fns)
+                        OTF_CUDA(cudaFuncSetAttribute((const void *)f,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)k.smem));
+                }
+        attrs_set = true;
+        return 0;
+    }
+};
+static KernelTable &ktable()
+{
+    static KernelTable t;
+    return t;
+}
+
+// ----------------------------------------------------------------- Engine
+
+Engine::~Engine() { free_all(); }
+
+void Engine::drop_graphs()
+{
+    if (g_fwd_)
+        cudaGraphExecDestroy(g_fwd_);
+    if (g_fwd_ring_)
+        cudaGraphExecDestroy(g_fwd_ring_);
+    if (g_rev_)
+        cudaGraphExecDestroy(g_rev_);
+    g_fwd_ = g_fwd_ring_ = g_rev_ = nullptr;
+    graph_shots_ = -1;
+}
+
+void Engine::free_all()
+{
+    drop_graphs();
+    if (qr_ == qf_)
+        qr_ = nullptr;  // aliased when dt == dx == 1: freed once, as qf_
+    float **fl[] = {&qf_, &qr_, &dampx_, &dampz_, &dampx2_, &dampz2_, &grad_, &rec_, &ring_,
+                    &src_, &tab_src_, &adj_, &tab_adj_};
+    for (float **p : fl) {
+        if (*p)
+            cudaFree(*p);
+        *p = nullptr;
+    }
+    for (auto &a : fld_)
+        for (auto &b : a)
+            for (auto &c : b) {
+                if (c)
+                    cudaFree(c);
+                c = nullptr;
+            }
+    int **il[] = {&inj_src_, &inj_adj_, &tabs_};
+    for (int **p : il) {
+        if (*p)
+            cudaFree(*p);
+        *p = nullptr;
+    }
+    if (st_)
+        cudaStreamDestroy(st_);
+    st_ = nullptr;
+    ready_ = false;
+    (void)cudaGetLastError();  // no stale runtime error may leak into the next launch check
+}
+
+int Engine::init(const EngineConfig &cfg, const float *d_x, const float *d_z)
+{
+    free_all();
+    OTF_CHECK(cfg.X >= 9 && cfg.Z >= 9, 1, "grid must be at least 9x9 cells");
+    OTF_CHECK(cfg.T >= 2, 1, "T must be at least 2");
+    OTF_CHECK(cfg.max_shots >= 1, 1, "max_shots must be >= 1");
+    OTF_CHECK(cfg.precision == kFaithful || cfg.precision == kFast, 1, "unknown precision");
+    OTF_CHECK(cfg.tile >= 0 && cfg.tile < kNumTileShapes, 1, "unknown tile shape");
+    OTF_CHECK(cfg.dx != 0.f, 1, "dx must be non-zero");
+    cfg_ = cfg;
+    L_ = Layout::make(cfg.X, cfg.Z);
+    const int X = cfg.X, Z = cfg.Z;
+    if (ktable().set_attrs())
+        return -1;
+    OTF_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+
+    // damping multipliers 1 - d*dt at the reference's +1-shifted index
+    // (d_x[z][x+1], d_z[z+1][x]: regression_PML_single.cu:505-506)
+    sep_ = true;
+    for (int z = 0; z < Z && sep_; z++)
+        for (int x = 0; x < X; x++)
+            if (d_x[(size_t)z * X + x] != d_x[x] || d_z[(size_t)z * X + x] != d_z[(size_t)z * X]) {
+                sep_ = false;
+                break;
+            }
+    const float dt = cfg.dt;
+    if (sep_) {
+        std::vector<float> hx(L_.pitch, 1.f), hz(L_.rows, 1.f);
+        for (int x = 0; x + 1 < X; x++)
+            hx[x + PAD] = std::fmaf(-d_x[x + 1], dt, 1.f);
+        for (int z = 0; z + 1 < Z; z++)
+            hz[z + PAD] = std::fmaf(-d_z[(size_t)(z + 1) * X], dt, 1.f);
+        OTF_CUDA(cudaMalloc(&dampx_, sizeof(float) * L_.pitch));
+        OTF_CUDA(cudaMalloc(&dampz_, sizeof(float) * L_.rows));
+        OTF_CUDA(cudaMemcpy(dampx_, hx.data(), sizeof(float) * L_.pitch, cudaMemcpyHostToDevice));
+        OTF_CUDA(cudaMemcpy(dampz_, hz.data(), sizeof(float) * L_.rows, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> hx(L_.slot, 1.f), hz(L_.slot, 1.f);
+        for (int z = 0; z < Z; z++)
+            for (int x = 0; x < X; x++) {
+                const size_t i = (size_t)z * X + x;
+                if (i + 1 < (size_t)X * Z)
+                    hx[L_.at(x, z)] = std::fmaf(-d_x[i + 1], dt, 1.f);
+                if (z + 1 < Z)
+                    hz[L_.at(x, z)] = std::fmaf(-d_z[i + X], dt, 1.f);
+            }
+        OTF_CUDA(cudaMalloc(&dampx2_, sizeof(float) * L_.slot));
+        OTF_CUDA(cudaMalloc(&dampz2_, sizeof(float) * L_.slot));
+        OTF_CUDA(cudaMemcpy(dampx2_, hx.data(), sizeof(float) * L_.slot, cudaMemcpyHostToDevice));
+        OTF_CUDA(cudaMemcpy(dampz2_, hz.data(), sizeof(float) * L_.slot, cudaMemcpyHostToDevice));
+        cfg_.tile = 0;  // the general-damping kernels are compiled for shape 0
+    }
+
+    two_q_ = !(cfg.dt == 1.f && cfg.dx == 1.f);
+    OTF_CUDA(cudaMalloc(&qf_, sizeof(float) * L_.slot));
+    OTF_CUDA(cudaMemset(qf_, 0, sizeof(float) * L_.slot));
+    if (two_q_) {
+        OTF_CUDA(cudaMalloc(&qr_, sizeof(float) * L_.slot));
+        OTF_CUDA(cudaMemset(qr_, 0, sizeof(float) * L_.slot));
+    } else {
+        qr_ = qf_;
+    }
+    const size_t fsz = sizeof(float) * (size_t)L_.slot * cfg.max_shots;
+    for (auto &a : fld_)
+        for (auto &b : a)
+            for (auto &c : b) {
+                OTF_CUDA(cudaMalloc(&c, fsz));
+                OTF_CUDA(cudaMemset(c, 0, fsz));
+            }
+    OTF_CUDA(cudaMalloc(&grad_, fsz));
+    OTF_CUDA(cudaMemset(grad_, 0, fsz));
+    ready_ = true;
+    return 0;
+}
+
+int Engine::set_precision(int prec)
+{
+    OTF_CHECK(prec == kFaithful || prec == kFast, 1, "unknown precision");
+    if (prec != cfg_.precision) {
+        cfg_.precision = prec;
+        drop_graphs();
+    }
+    return 0;
+}
+
+int Engine::set_tile(int tile)
+{
+    OTF_CHECK(tile >= 0 && tile < kNumTileShapes, 1, "unknown tile shape");
+    if (!sep_)
+        tile = 0;
+    if (tile != cfg_.tile) {
+        cfg_.tile = tile;
+        tables_dirty_ = true;
+        drop_graphs();
+    }
+    return 0;
+}
+
+int Engine::set_model(const float *cquad, bool on_device)
+{
+    OTF_CHECK(ready_, 2, "engine not initialised");
+    const size_t n = (size_t)cfg_.X * cfg_.Z;
+    float *tmp = nullptr;
+    const float *dsrc = cquad;
+    if (!on_device) {
+        OTF_CUDA(cudaMallocAsync(&tmp, sizeof(float) * n, st_));
+        OTF_CUDA(cudaMemcpyAsync(tmp, cquad, sizeof(float) * n, cudaMemcpyHostToDevice, st_));
+        dsrc = tmp;
+    }
+    const int bs = 256;
+    const int nb = (int)((L_.slot + bs - 1) / bs);
+    k_prep_q<<<nb, bs, 0, st_>>>(dsrc, qf_, two_q_ ? qr_ : nullptr, L_, cfg_.dx, cfg_.dt);
+    OTF_CUDA(cudaGetLastError());
+    if (tmp)
+        OTF_CUDA(cudaFreeAsync(tmp, st_));
+    return 0;
+}
+
+static bool inside(int x, int z, int X, int Z) { return x >= 0 && z >= 0 && x < X && z < Z; }
+static bool interior(int x, int z, int X, int Z) { return x >= 4 && z >= 4 && x < X - 4 && z < Z - 4; }
+
+int Engine::set_sources(int n, const int *x, const int *z, const float *src)
+{
+    OTF_CHECK(ready_, 2, "engine not initialised");
+    OTF_CHECK(n >= 0, 1, "negative source count");
+    for (int k = 0; k < n; k++)
+        OTF_CHECK(interior(x[k], z[k], cfg_.X, cfg_.Z), 3,
+                  "source " + std::to_string(k) + " at (" + std::to_string(x[k]) + "," +
+                      std::to_string(z[k]) + ") is outside the updated region 4 <= x < X-4, 4 <= z < Z-4");
+    src_x_.assign(x, x + n);
+    src_z_.assign(z, z + n);
+    n_src_ = n;
+    if (src_)
+        cudaFree(src_);
+    if (tab_src_)
+        cudaFree(tab_src_);
+    src_ = tab_src_ = nullptr;
+    const size_t sz = sizeof(float) * (size_t)std::max(n, 1) * cfg_.T;
+    OTF_CUDA(cudaMalloc(&src_, sz));
+    OTF_CUDA(cudaMalloc(&tab_src_, sz));
+    OTF_CUDA(cudaMemset(tab_src_, 0, sz));
+    if (n > 0) {
+        OTF_CUDA(cudaMemcpyAsync(src_, src, sizeof(float) * (size_t)n * cfg_.T,
+                                 cudaMemcpyHostToDevice, st_));
+        k_prefix_rows<<<(n + 127) / 128, 128, 0, st_>>>(src_, tab_src_, n, cfg_.T, 0);
+        OTF_CUDA(cudaGetLastError());
+    }
+    tables_dirty_ = true;
+    drop_graphs();
+    return 0;
+}
+
+int Engine::set_receivers(int n, const int *x, const int *z)
+{
+    OTF_CHECK(ready_, 2, "engine not initialised");
+    OTF_CHECK(n >= 0, 1, "negative receiver count");
+    // A receiver may sit on a never-updated cell (within 4 cells of the
+    // edge): it records zeros, as in the reference, and takes no part in the
+    // adjoint injection (the reference injects there into a cell no stencil reads).
+    for (int k = 0; k < n; k++)
+        OTF_CHECK(inside(x[k], z[k], cfg_.X, cfg_.Z), 3,
+                  "receiver " + std::to_string(k) + " at (" + std::to_string(x[k]) + "," +
+                      std::to_string(z[k]) + ") is outside the grid");
+    rec_x_.assign(x, x + n);
+    rec_z_.assign(z, z + n);
+    n_rec_ = n;
+    float **bufs[] = {&rec_, &adj_, &tab_adj_};
+    for (float **b : bufs) {
+        if (*b)
+            cudaFree(*b);
+        *b = nullptr;
+    }
+    const size_t sz = sizeof(float) * (size_t)std::max(n, 1) * cfg_.T * cfg_.max_shots;
+    for (float **b : bufs) {
+        OTF_CUDA(cudaMalloc(b, sz));
+        OTF_CUDA(cudaMemset(*b, 0, sz));
+    }
+    tables_dirty_ = true;
+    drop_graphs();
+    return 0;
+}
+
+int Engine::set_ring(int n, const int *x, const int *z)
+{
+    OTF_CHECK(ready_, 2, "engine not initialised");
+    OTF_CHECK(n >= 0, 1, "negative ring size");
+    for (int k = 0; k < n; k++)
+        OTF_CHECK(interior(x[k], z[k], cfg_.X, cfg_.Z), 3,
+                  "ring cell " + std::to_string(k) + " is outside the updated region");
+    ring_x_.assign(x, x + n);
+    ring_z_.assign(z, z + n);
+    n_ring_ = n;
+    if (ring_)
+        cudaFree(ring_);
+    ring_ = nullptr;
+    const size_t sz = sizeof(float) * (size_t)std::max(n, 1) * cfg_.T * cfg_.max_shots;
+    OTF_CUDA(cudaMalloc(&ring_, sz));
+    OTF_CUDA(cudaMemset(ring_, 0, sz));
+    tables_dirty_ = true;
+    drop_graphs();
+    return 0;
+}
+
+int Engine::set_shots(int n_shots, const int *ptr, const int *srcs)
+{
+    OTF_CHECK(ready_, 2, "engine not initialised");
+    OTF_CHECK(n_shots >= 1 && n_shots <= cfg_.max_shots, 1, "shot count out of range");
+    for (int s = 0; s < n_shots; s++)
+        OTF_CHECK(ptr[s] <= ptr[s + 1], 1, "shot table not monotone");
+    for (int k = ptr[0]; k < ptr[n_shots]; k++)
+        OTF_CHECK(srcs[k] >= 0 && srcs[k] < n_src_, 1, "shot references an unknown source");
+    // capacity of the injection table: every shot may fire every source once
+    const size_t cap = (size_t)std::max(n_src_, 1) * cfg_.max_shots;
+    OTF_CHECK((size_t)(ptr[n_shots] - ptr[0]) <= cap, 1, "too many source firings in the shot table");
+    shot_ptr_.assign(ptr, ptr + n_shots + 1);
+    for (auto &v : shot_ptr_)
+        v -= ptr[0];
+    shot_srcs_.assign(srcs + ptr[0], srcs + ptr[n_shots]);
+    if (n_shots != n_shots_) {
+        drop_graphs();
+        tables_dirty_ = true;  // the adjoint injection table is sized by the shot count
+    }
+    n_shots_ = n_shots;
+
+    // forward injection CSR in a fixed layout (so captured graphs stay valid
+    // when only the firing pattern changes): ptr[max_shots+1] | x[cap] | z[cap] | row[cap]
+    const size_t np = (size_t)cfg_.max_shots + 1;
+    std::vector<int> h(np + 3 * cap, 0);
+    std::copy(shot_ptr_.begin(), shot_ptr_.end(), h.begin());
+    int *hx = h.data() + np, *hz = hx + cap, *hr = hz + cap;
+    for (size_t k = 0; k < shot_srcs_.size(); k++) {
+        hx[k] = src_x_[shot_srcs_[k]];
+        hz[k] = src_z_[shot_srcs_[k]];
+        hr[k] = shot_srcs_[k];
+    }
+    if (h.size() != inj_src_cap_) {
+        if (inj_src_)
+            cudaFree(inj_src_);
+        inj_src_ = nullptr;
+        OTF_CUDA(cudaMalloc(&inj_src_, sizeof(int) * h.size()));
+        inj_src_cap_ = h.size();
+        drop_graphs();
+    }
+    OTF_CUDA(cudaMemcpyAsync(inj_src_, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, st_));
+    OTF_CUDA(cudaStreamSynchronize(st_));
+    inj_src_ptr_ = inj_src_;
+    inj_src_x_ = inj_src_ + np;
+    inj_src_z_ = inj_src_x_ + cap;
+    inj_src_row_ = inj_src_z_ + cap;
+    return 0;
+}
+
+// Per-tile receiver / ring tables and the adjoint injection table; depend on
+// the tile shape and the point sets.
+int Engine::build_tables()
+{
+    const TileShape ts = kTileShapes[cfg_.tile];
+    const int TX = ts.tx, TZ = ts.tz, X = cfg_.X, Z = cfg_.Z;
+    const int ntx = (X + TX - 1) / TX, ntz = (Z + TZ - 1) / TZ, ntiles = ntx * ntz;
+    const int EX = TX + 8;
+    auto owned = [&](int x, int z, int &tile, int &cell) {
+        tile = (z / TZ) * ntx + x / TX;
+        cell = (z % TZ) * TX + x % TX;
+    };
+    std::vector<std::vector<std::pair<int, int>>> sen(ntiles), ringo(ntiles), ringe(ntiles);
+    for (int n = 0; n < n_rec_; n++) {
+        int tl, c;
+        owned(rec_x_[n], rec_z_[n], tl, c);
+        sen[tl].push_back({c, n});
+    }
+    for (int n = 0; n < n_ring_; n++) {
+        int tl, c;
+        owned(ring_x_[n], ring_z_[n], tl, c);
+        ringo[tl].push_back({c, n});
+    }
+    std::vector<int> h;
+    auto flatten = [&](std::vector<std::vector<std::pair<int, int>>> &v, bool with_id,
+                       std::vector<int> &ids_out) {
+        std::vector<int> ptr(ntiles + 1, 0), cell, id;
+        for (int tl = 0; tl < ntiles; tl++) {
+            ptr[tl + 1] = ptr[tl] + (int)v[tl].size();
+            for (auto &e : v[tl]) {
+                cell.push_back(e.first);
+                id.push_back(e.second);
+            }
+        }
+        const size_t off = h.size();
+        h.insert(h.end(), ptr.begin(), ptr.end());
+        h.insert(h.end(), cell.begin(), cell.end());
+        h.push_back(0);
+        if (with_id) {
+            h.insert(h.end(), id.begin(), id.end());
+            h.push_back(0);
+        }
+        ids_out = id;
+        return off;
+    };
+    std::vector<int> sen_ids, ring_order, dummy;
+    const size_t o_sen = h.size();
+    flatten(sen, true, sen_ids);
+    const size_t o_ringo = h.size();
+    flatten(ringo, false, ring_order);
+    // internal ring id of reference ring index n = its position in ring_order
+    std::vector<int> ring_id(n_ring_);
+    for (int e = 0; e < (int)ring_order.size(); e++)
+        ring_id[ring_order[e]] = e;
+    for (int n = 0; n < n_ring_; n++) {
+        const int x = ring_x_[n], z = ring_z_[n];
+        for (int tz = std::max(0, (z - 4) / TZ - 1); tz <= std::min(ntz - 1, (z + 4) / TZ + 1); tz++)
+            for (int tx = std::max(0, (x - 4) / TX - 1); tx <= std::min(ntx - 1, (x + 4) / TX + 1); tx++) {
+                const int ex = x - (tx * TX - 4), ez = z - (tz * TZ - 4);
+                if (ex >= 0 && ex < EX && ez >= 0 && ez < TZ + 8)
+                    ringe[tz * ntx + tx].push_back({ez * EX + ex, ring_id[n]});
+            }
+    }
+    const size_t o_ringe = h.size();
+    flatten(ringe, true, dummy);
+
+    // adjoint injection: every receiver of shot s with tab row s*n_rec + n
+    const size_t o_adj = h.size();
+    {
+        const int ni = n_rec_ * n_shots_;
+        h.reserve(h.size() + n_shots_ + 1 + 3 * (size_t)ni);
+        for (int s = 0; s <= n_shots_; s++)
+            h.push_back(s * n_rec_);
+        for (int s = 0; s < n_shots_; s++)
+            for (int n = 0; n < n_rec_; n++)  // off-grid x disables injection at edge receivers
+                h.push_back(interior(rec_x_[n], rec_z_[n], X, Z) ? rec_x_[n] : -(1 << 20));
+        for (int s = 0; s < n_shots_; s++)
+            for (int n = 0; n < n_rec_; n++)
+                h.push_back(rec_z_[n]);
+        for (int s = 0; s < n_shots_; s++)
+            for (int n = 0; n < n_rec_; n++)
+                h.push_back(s * n_rec_ + n);
+    }
+    if (h.size() > tabs_cap_) {
+        if (tabs_)
+            cudaFree(tabs_);
+        OTF_CUDA(cudaMalloc(&tabs_, sizeof(int) * h.size()));
+        tabs_cap_ = h.size();
+    }
+    OTF_CUDA(cudaMemcpyAsync(tabs_, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, st_));
+    OTF_CUDA(cudaStreamSynchronize(st_));
+    int *d = tabs_;
+    sen_ptr_ = d + o_sen;
+    sen_cell_ = sen_ptr_ + ntiles + 1;
+    sen_id_ = sen_cell_ + n_rec_ + 1;
+    ringo_ptr_ = d + o_ringo;
+    ringo_cell_ = ringo_ptr_ + ntiles + 1;
+    ringe_ptr_ = d + o_ringe;
+    {
+        int ne = 0;
+        for (auto &v : ringe)
+            ne += (int)v.size();
+        ringe_cell_ = ringe_ptr_ + ntiles + 1;
+        ringe_id_ = ringe_cell_ + ne + 1;
+    }
+    inj_adj_ptr_ = d + o_adj;
+    inj_adj_x_ = inj_adj_ptr_ + n_shots_ + 1;
+    inj_adj_z_ = inj_adj_x_ + n_rec_ * n_shots_;
+    inj_adj_row_ = inj_adj_z_ + n_rec_ * n_shots_;
+    tables_dirty_ = false;
+    drop_graphs();
+    return 0;
+}
+
+StepParams Engine::base_params() const
+{
+    const TileShape ts = kTileShapes[cfg_.tile];
+    StepParams p;
+    memset(&p, 0, sizeof(p));
+    p.X = cfg_.X;
+    p.Z = cfg_.Z;
+    p.pitch = L_.pitch;
+    p.rows = L_.rows;
+    p.T = cfg_.T;
+    p.ntx = (cfg_.X + ts.tx - 1) / ts.tx;
+    p.shot_stride = L_.slot;
+    p.r = cfg_.dt / cfg_.dx;
+    p.dampx = dampx_;
+    p.dampz = dampz_;
+    p.dampx2 = dampx2_;
+    p.dampz2 = dampz2_;
+    p.sen_ptr = sen_ptr_;
+    p.sen_cell = sen_cell_;
+    p.sen_id = sen_id_;
+    p.rec = rec_;
+    p.n_sen = n_rec_;
+    p.ringo_ptr = ringo_ptr_;
+    p.ringo_cell = ringo_cell_;
+    p.ringe_ptr = ringe_ptr_;
+    p.ringe_cell = ringe_cell_;
+    p.ringe_id = ringe_id_;
+    p.ring = ring_;
+    p.n_ring = n_ring_;
+    p.grad = grad_;
+    return p;
+}
+
+int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid)
+{
+    const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
+    void *args[] = {(void *)&p};
+    OTF_CUDA(cudaLaunchKernel((const void *)(with_ring ? k.fwd_ring : k.fwd), grid, dim3(NT),
+                              args, k.smem, st_));
+    return 0;
+}
+
+int Engine::launch_reverse_step(const StepParams &p, dim3 grid)
+{
+    const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
+    void *args[] = {(void *)&p};
+    OTF_CUDA(cudaLaunchKernel((const void *)k.rev, grid, dim3(NT), args, k.smem, st_));
+    return 0;
+}
+
+static dim3 step_grid(const EngineConfig &c, int n_shots)
+{
+    const TileShape ts = kTileShapes[c.tile];
+    const int ntx = (c.X + ts.tx - 1) / ts.tx, ntz = (c.Z + ts.tz - 1) / ts.tz;
+    return dim3((unsigned)(ntx * ntz), (unsigned)n_shots, 1);
+}
+
+int Engine::capture_forward(bool with_ring, cudaGraphExec_t *out)
+{
+    StepParams p = base_params();
+    p.q0 = qf_;
+    p.q1 = qf_;
+    p.inj_ptr = inj_src_ptr_;
+    p.inj_x = inj_src_x_;
+    p.inj_z = inj_src_z_;
+    p.inj_row = inj_src_row_;
+    p.inj_tab = tab_src_;
+    const dim3 grid = step_grid(cfg_, n_shots_);
+    const size_t fbytes = sizeof(float) * (size_t)L_.slot * n_shots_;
+    cudaGraph_t g = nullptr;
+    OTF_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    for (int f = 0; f < 4 && !rc; f++)
+        for (int s = 0; s < 2 && !rc; s++)
+            if (cudaMemsetAsync(fld_[0][f][s], 0, fbytes, st_) != cudaSuccess)
+                rc = -1;
+    for (int t = 1; t < cfg_.T && !rc; t++) {
+        const int i = (t - 1) & 1, o = t & 1;
+        p.t = t;
+        p.f0 = Fields{fld_[0][0][i], fld_[0][1][i], fld_[0][2][i], fld_[0][3][i],
+                      fld_[0][0][o], fld_[0][1][o], fld_[0][2][o], fld_[0][3][o]};
+        rc = launch_forward_step(p, with_ring, grid);
+    }
+    const cudaError_t ec = cudaStreamEndCapture(st_, &g);
+    if (rc)
+        return rc;
+    OTF_CUDA(ec);
+    const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    OTF_CUDA(ei);
+    return 0;
+}
+
+int Engine::capture_reverse(cudaGraphExec_t *out)
+{
+    StepParams p = base_params();
+    p.q0 = qr_;
+    p.q1 = qf_;
+    p.inj_ptr = inj_adj_ptr_;
+    p.inj_x = inj_adj_x_;
+    p.inj_z = inj_adj_z_;
+    p.inj_row = inj_adj_row_;
+    p.inj_tab = tab_adj_;
+    const dim3 grid = step_grid(cfg_, n_shots_);
+    const size_t fbytes = sizeof(float) * (size_t)L_.slot * n_shots_;
+    const int T = cfg_.T;
+    cudaGraph_t g = nullptr;
+    OTF_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    for (int f = 0; f < 4 && !rc; f++)
+        for (int s = 0; s < 2 && !rc; s++)
+            if (cudaMemsetAsync(fld_[1][f][s], 0, fbytes, st_) != cudaSuccess)
+                rc = -1;
+    if (!rc && cudaMemsetAsync(grad_, 0, fbytes, st_) != cudaSuccess)
+        rc = -1;
+    for (int t = 1; t < T && !rc; t++) {
+        // reconstruction starts from P(T-1) (slot (T-1)%2) and A(T-2)
+        // (slot (T-2)%2) (regression_PML_single.cu:787-790) and ping-pongs
+        const int pi = (T + t) & 1, po = (T + t + 1) & 1;
+        const int ai = (T + t + 1) & 1, ao = (T + t) & 1;
+        const int i = (t - 1) & 1, o = t & 1;
+        p.t = t;
+        p.f0 = Fields{fld_[0][0][pi], fld_[0][1][pi], fld_[0][2][ai], fld_[0][3][ai],
+                      fld_[0][0][po], fld_[0][1][po], fld_[0][2][ao], fld_[0][3][ao]};
+        p.f1 = Fields{fld_[1][0][i], fld_[1][1][i], fld_[1][2][i], fld_[1][3][i],
+                      fld_[1][0][o], fld_[1][1][o], fld_[1][2][o], fld_[1][3][o]};
+        rc = launch_reverse_step(p, grid);
+    }
+    const cudaError_t ec = cudaStreamEndCapture(st_, &g);
+    if (rc)
+        return rc;
+    OTF_CUDA(ec);
+    const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    OTF_CUDA(ei);
+    return 0;
+}
+
+int Engine::forward(bool with_ring)
+{
+    OTF_CHECK(ready_, 2, "engine not initialised");
+    OTF_CHECK(!shot_ptr_.empty(), 2, "no shots configured");
+    if (tables_dirty_ && build_tables())
+        return -1;
+    cudaGraphExec_t *g = with_ring ? &g_fwd_ring_ : &g_fwd_;
+    if (!*g && capture_forward(with_ring, g))
+        return -1;
+    OTF_CUDA(cudaGraphLaunch(*g, st_));
+    return 0;
+}
+
+int Engine::reverse()
+{
+    OTF_CHECK(ready_, 2, "engine not initialised");
+    if (tables_dirty_ && build_tables())
+        return -1;
+    const int rows = n_rec_ * n_shots_;
+    if (rows > 0) {
+        k_prefix_rows<<<(rows + 127) / 128, 128, 0, st_>>>(adj_, tab_adj_, rows, cfg_.T, 1);
+        OTF_CUDA(cudaGetLastError());
+    }
+    if (!g_rev_ && capture_reverse(&g_rev_))
+        return -1;
+    OTF_CUDA(cudaGraphLaunch(g_rev_, st_));
+    return 0;
+}
+
+int Engine::copy_traces(float *dst, int shot0, int n, cudaMemcpyKind kind)
+{
+    const size_t per = (size_t)n_rec_ * cfg_.T;
+    OTF_CUDA(cudaMemcpyAsync(dst, rec_ + per * shot0, sizeof(float) * per * n, kind, st_));
+    return 0;
+}
+
+int Engine::copy_grad_shot(int shot, float *dst, cudaMemcpyKind kind)
+{
+    const float *src = grad_ + L_.slot * shot + L_.at(0, 0);
+    OTF_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * cfg_.X, src, sizeof(float) * L_.pitch,
+                               sizeof(float) * cfg_.X, cfg_.Z, kind, st_));
+    return 0;
+}
+
+int Engine::grad_sum(float *dst, float scale)
+{
+    const int64_t n = (int64_t)cfg_.X * cfg_.Z;
+    k_grad_sum<<<(unsigned)((n + 255) / 256), 256, 0, st_>>>(grad_, dst, L_, n_shots_, L_.slot, scale);
+    OTF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int Engine::sync()
+{
+    OTF_CUDA(cudaStreamSynchronize(st_));
+    return 0;
+}
+
+}  // namespace otf

@@ -1,0 +1,115 @@
+// Host-side engine: owns the device state of one problem (grid, model,
+// receivers, sources, boundary ring) for a batch of shots and drives the
+// fused step kernels through captured CUDA graphs.
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+#include "otf_common.cuh"
+#include "pml_step.cuh"
+
+namespace otf {
+
+enum Precision : int { kFaithful = 0, kFast = 1 };
+
+// Tile shapes compiled into the library (owned cells per CTA).
+struct TileShape {
+    int tx, tz;
+};
+constexpr int kNumTileShapes = 4;
+extern const TileShape kTileShapes[kNumTileShapes];
+
+struct EngineConfig {
+    int X = 0, Z = 0, T = 0;
+    float dx = 1.f, dz = 1.f, dt = 1.f;  // the reference's constvec {dx, dz, dt}
+    int max_shots = 1;
+    int precision = kFaithful;
+    int tile = 0;  // index into kTileShapes
+};
+
+class Engine {
+  public:
+    Engine() = default;
+    ~Engine();
+    Engine(const Engine &) = delete;
+    Engine &operator=(const Engine &) = delete;
+
+    // Set-up. All host arrays; d_x / d_z are [Z*X] damping profiles as the
+    // reference takes them (cuda_interface_pml.py:116-132 builds them).
+    int init(const EngineConfig &cfg, const float *d_x, const float *d_z);
+    int set_model(const float *cquad, bool on_device);  // c^2 in the reference's nondimensional units, [Z*X]
+    int set_sources(int n, const int *x, const int *z, const float *src);  // src [n*T]
+    int set_receivers(int n, const int *x, const int *z);
+    int set_ring(int n, const int *x, const int *z);
+    // Which sources fire in each shot: shot s fires srcs[ptr[s] .. ptr[s+1]).
+    int set_shots(int n_shots, const int *ptr, const int *srcs);
+
+    // Forward modelling of all shots; receivers recorded into rec_dev()
+    // ([n_shots][n_rec][T], column 0 zero). With ring, the boundary ring is
+    // recorded too (gradient phase 1).
+    int forward(bool with_ring);
+    // Reverse phase of the gradient (phase 2) given adjoint sources already in
+    // adj_dev() ([n_shots][n_rec][T]); per-shot gradients land in grad_dev().
+    int reverse();
+
+    // Copies of results.
+    int copy_traces(float *dst, int shot0, int n, cudaMemcpyKind kind);
+    int copy_grad_shot(int shot, float *dst, cudaMemcpyKind kind);  // unpadded [Z*X]
+    int grad_sum(float *dst_dev_unpadded, float scale);             // sum over shots * scale
+
+    float *rec_dev() { return rec_; }
+    float *adj_dev() { return adj_; }
+    cudaStream_t stream() const { return st_; }
+    int n_shots() const { return n_shots_; }
+    int n_rec() const { return n_rec_; }
+    const EngineConfig &config() const { return cfg_; }
+    const Layout &layout() const { return L_; }
+    int set_precision(int prec);
+    int set_tile(int tile);
+    int sync();
+
+  private:
+    int build_tables();
+    int capture_forward(bool with_ring, cudaGraphExec_t *out);
+    int capture_reverse(cudaGraphExec_t *out);
+    int launch_forward_step(const StepParams &p, bool with_ring, dim3 grid);
+    int launch_reverse_step(const StepParams &p, dim3 grid);
+    void drop_graphs();
+    StepParams base_params() const;
+    void free_all();
+
+    EngineConfig cfg_;
+    Layout L_;
+    bool ready_ = false;
+    bool sep_ = true;
+    bool two_q_ = false;
+    int n_src_ = 0, n_rec_ = 0, n_ring_ = 0, n_shots_ = 1;
+    std::vector<int> src_x_, src_z_, rec_x_, rec_z_, ring_x_, ring_z_;
+    std::vector<int> shot_ptr_, shot_srcs_;
+
+    cudaStream_t st_ = nullptr;
+    // device buffers
+    float *qf_ = nullptr, *qr_ = nullptr;                            // padded P coefficients
+    float *dampx_ = nullptr, *dampz_ = nullptr;                      // separable multipliers
+    float *dampx2_ = nullptr, *dampz2_ = nullptr;                    // general multipliers
+    float *fld_[2][4][2] = {};  // [set][Px,Pz,Ax,Az][slot], each [max_shots][slot floats]
+    float *grad_ = nullptr;     // [max_shots][slot floats]
+    float *rec_ = nullptr;      // [max_shots][n_rec][T]
+    float *ring_ = nullptr;     // [max_shots][T][n_ring]
+    float *src_ = nullptr, *tab_src_ = nullptr;  // [n_src][T]
+    float *adj_ = nullptr, *tab_adj_ = nullptr;  // [max_shots][n_rec][T]
+    int *inj_src_ = nullptr;   // CSR: ptr[max_shots+1] | x | z | row
+    int *inj_adj_ = nullptr;
+    int *tabs_ = nullptr;      // per-tile receiver / ring tables
+    size_t inj_src_cap_ = 0, tabs_cap_ = 0;
+    int *sen_ptr_ = nullptr, *sen_cell_ = nullptr, *sen_id_ = nullptr;
+    int *ringo_ptr_ = nullptr, *ringo_cell_ = nullptr;
+    int *ringe_ptr_ = nullptr, *ringe_cell_ = nullptr, *ringe_id_ = nullptr;
+    int *inj_src_ptr_ = nullptr, *inj_src_x_ = nullptr, *inj_src_z_ = nullptr, *inj_src_row_ = nullptr;
+    int *inj_adj_ptr_ = nullptr, *inj_adj_x_ = nullptr, *inj_adj_z_ = nullptr, *inj_adj_row_ = nullptr;
+
+    cudaGraphExec_t g_fwd_ = nullptr, g_fwd_ring_ = nullptr, g_rev_ = nullptr;
+    int graph_shots_ = -1;
+    bool tables_dirty_ = true;
+};
+
+}  // namespace otf

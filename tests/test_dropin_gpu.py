@@ -1,0 +1,154 @@
+"""GPU parity of the drop-in C ABI (libotfwi.so) against the reference
+library's own outputs (tests/golden/sim_*.npz) and the CPU oracle, through
+the reference wrapper's call sequence (tests/abi_driver.py).
+
+Faithful mode (the default) restates the reference's arithmetic operation by
+operation, so it is required to be bit-identical to the reference library
+and to the f32 oracle: traces (t >= 1) and gradients, every sample.
+Against the FP64 oracle, and for the fast (FP32-sum) mode, the error
+measures are: traces -- max over receivers of max_{t>=1}|d| / max_t|ref|
+(tolerance 1e-5 faithful, 1e-4 fast); gradients -- relative L2 over the grid
+(1e-4 faithful, 1e-3 fast).
+"""
+import glob
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+from abi_driver import run_abi  # noqa: E402
+from test_oracle import oracle_case, rel_l2, rel_trace_err  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    import make_sim_golden
+    return make_sim_golden.cases()
+
+
+def _run(lib, inp, precision=0, tile=0):
+    from otfwi_b200 import _lib
+    os.environ["OTFWI_PRECISION"] = str(precision)
+    os.environ["OTFWI_TILE"] = str(tile)
+    try:
+        return run_abi(lib, **inp, check=lambda: _lib.check(lib))
+    finally:
+        os.environ.pop("OTFWI_PRECISION", None)
+        os.environ.pop("OTFWI_TILE", None)
+
+
+def _keys(ref):
+    return [k for k in ref if k.startswith(("traces_", "sim_s", "grad_s"))]
+
+
+def _assert_identical(res, ref, label):
+    for k in _keys(ref):
+        a, b = np.asarray(res[k]), np.asarray(ref[k])
+        if not k.startswith("grad_s"):
+            a, b = a[:, 1:], b[:, 1:]  # column 0 is never simulated
+        nd = int(np.sum(a != b))
+        assert nd == 0, (label, k, nd, a.size)
+
+
+def _assert_close(res, ref, ttol, gtol, label):
+    errs = {}
+    for k in _keys(ref):
+        if k.startswith("grad_s"):
+            errs[k] = rel_l2(res[k], ref[k])
+            assert errs[k] <= gtol, (label, k, errs[k])
+        else:
+            errs[k] = rel_trace_err(res[k], ref[k])
+            assert errs[k] <= ttol, (label, k, errs[k])
+    return errs
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "sim_*.npz"))),
+                         ids=os.path.basename)
+def test_dropin_bit_identical_to_reference_library(lib, path):
+    d = dict(np.load(path))
+    _assert_identical(_run(lib, d), d, "faithful vs reference library")
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "sim_*.npz"))),
+                         ids=os.path.basename)
+def test_fast_mode_close_to_reference_library(lib, path):
+    d = dict(np.load(path))
+    errs = _assert_close(_run(lib, d, precision=1), d, 1e-4, 1e-3, "fast vs reference library")
+    print(os.path.basename(path), {k: f"{v:.2e}" for k, v in errs.items()})
+
+
+@pytest.mark.parametrize("name", ["small", "medium", "general"])
+def test_dropin_matches_oracles(lib, name):
+    inp = _cases()[name]
+    res = _run(lib, inp)
+    _assert_identical(res, oracle_case(inp, "f32"), "faithful vs oracle f32")
+    _assert_close(res, oracle_case(inp, "f64"), 1e-5, 1e-4, "faithful vs oracle f64")
+
+
+@pytest.mark.parametrize("tile", [1, 2, 3])
+def test_tile_shapes_bit_identical(lib, tile):
+    inp = _cases()["medium"]
+    base = _run(lib, inp, tile=0)
+    res = _run(lib, inp, tile=tile)
+    for k in base:
+        assert np.array_equal(base[k], res[k]), (tile, k)
+
+
+def test_odd_grid_sizes_every_tile(lib):
+    """Grids that are not multiples of any tile shape."""
+    import make_sim_golden
+    from otfwi_b200 import scenarios
+    from otfwi_b200.cuda_interface_pml import pml_damping
+    sc = scenarios.small(X=101, Z=77, T=200, n_src=1, n_rec=5, seed=3)
+    inp = make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))
+    ref = oracle_case(inp, "f32")
+    for tile in range(4):
+        _assert_identical(_run(lib, inp, tile=tile), ref, f"odd grid tile {tile}")
+
+
+def test_edge_receiver_records_zero(lib):
+    """A receiver on a never-updated cell (within 4 cells of the edge) records
+    zeros, as in the reference."""
+    import make_sim_golden
+    from otfwi_b200 import scenarios
+    from otfwi_b200.cuda_interface_pml import pml_damping
+    sc = scenarios.small(X=96, Z=64, T=150, n_src=1, n_rec=4, seed=2)
+    sc.rec_mask[sc.PML + 6, 2] = True  # x = 2: outside 4 <= x < X-4
+    inp = make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))
+    res = _run(lib, inp)
+    assert np.all(res["traces_all"][0] == 0.0)
+    assert np.abs(res["traces_all"][1:]).max() > 0
+
+
+def test_invalid_source_position_is_reported(lib):
+    from otfwi_b200 import _lib
+    import make_sim_golden
+    from otfwi_b200 import scenarios
+    from otfwi_b200.cuda_interface_pml import pml_damping
+    sc = scenarios.small(X=96, Z=64, T=50, n_src=1, n_rec=4, seed=2)
+    sc.src_mask[:] = False
+    sc.src_mask[2, 40] = True  # z = 2: a cell the scheme never updates
+    inp = make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))
+    with pytest.raises(_lib.OtfwiError, match="source 0"):
+        _run(lib, inp)
+
+
+def test_hilbert_matches_fft_definition(lib):
+    from otfwi_b200._lib import c_float_p
+    rng = np.random.default_rng(0)
+    for N in (64, 101, 500):
+        x = rng.standard_normal(N).astype(np.float32)
+        s90 = np.zeros(N, np.float32)
+        env = np.zeros(N, np.float32)
+        lib.hilbert(x.ctypes.data_as(c_float_p), s90.ctypes.data_as(c_float_p),
+                    env.ctypes.data_as(c_float_p), N)
+        X = np.fft.fft(x.astype(np.float64))
+        X[N // 2: 2 * (N // 2)] = 0
+        y = np.fft.ifft(X) * N
+        assert np.allclose(s90, 2 * y.imag / N, atol=1e-5)
+        assert np.allclose(env, 2 * np.abs(y) / N, atol=1e-5)
