@@ -1,0 +1,379 @@
+"""Benchmark: batched full-matrix-capture forward + adjoint gradient.
+
+Workload (one "step"): one complete FWI gradient of a 64-element
+full-matrix-capture acquisition on a 512 x 512 grid, T = 4000 time steps,
+20-cell PML, 64 shots x 64 receivers, quadratic Wasserstein misfit on
+softplus-normalised traces: forward modelling of all 64 shots with boundary
+ring recording, device misfit and adjoint sources, adjoint + reconstruction
++ imaging condition for all shots, shot mean of the gradient. Synthetic,
+seeded model (5900 m/s with three 3000 m/s circular defects) and 5 MHz
+Ricker source; the gradient is taken at the homogeneous starting model
+against data simulated from the true model.
+
+Metric: fwd+adj Gcell-steps/s = 2 * X * Z * (T-1) * shots / step time
+(whole job over all ranks). Run: python bench.py [--gpus N --steps K --warmup W]
+or --impl reference for the reference library's per-shot loop.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+adj Gcell-steps/s"
+UNIT = "Gcell-steps/s"
+# algorithmic HBM bytes per cell per time step (one shot): forward 28
+# (P, Ax, Az read + write, c^2 read), adjoint 28, reconstruction 28, gradient
+# read + write 8 -> 92; the reverse step kernel carries 64 of them, the forward 28
+BYTES_FWD = 28
+BYTES_REV = 64
+BYTES_STEP = 92
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", type=int, default=int(os.environ.get("OTFWI_BENCH_PRECISION", "1")))
+    ap.add_argument("--tile", type=int, default=int(os.environ.get("OTFWI_BENCH_TILE", "0")))
+    ap.add_argument("--X", type=int, default=512)
+    ap.add_argument("--T", type=int, default=4000)
+    ap.add_argument("--shots", type=int, default=64)
+    ap.add_argument("--misfit", default="wasserstein_softplus")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-shots", type=int, default=2, help="shots per reference-arm step")
+    return ap.parse_args()
+
+
+def workload(args):
+    from otfwi_b200 import scenarios
+    return scenarios.fmc(X=args.X, Z=args.X, T=args.T, n_elem=args.shots,
+                         x_first=max(24, args.X // 2 - 3 * args.shots + 3))
+
+
+def config_block(args, sc, parallelism):
+    return {"workload": f"fmc{sc.X}x{sc.Z}_T{sc.T}_{sc.n_src}shots_{sc.n_rec}rx_{args.misfit}",
+            "grid": [sc.X, sc.Z], "nt": sc.T, "pml": sc.PML, "shots": sc.n_src, "receivers": sc.n_rec,
+            "misfit": args.misfit, "precision": ["faithful", "fast"][args.precision],
+            "l2": "working set (fields of 64 shots, about 1.2 GB) larger than the 126 MB L2; no flush needed",
+            "parallelism": parallelism}
+
+
+class Clocks:
+    """Samples nvidia-smi during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per cell of one reverse-step launch from the committed ncu
+    summary (profiles/reverse_step_fmc.md, line 'dram_bytes_per_cell: N')."""
+    p = os.path.join(ROOT, "profiles", "reverse_step_fmc.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_cell:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def cpu_baseline(args, sc):
+    """FP64 oracle (C, OpenMP, all host threads) on a bounded sample: one shot
+    of the same FMC problem, the first T_s time steps, forward + misfit +
+    adjoint gradient; rate in the metric's unit."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pml_oracle as po
+    import misfit_oracle as mo
+    from otfwi_b200.cuda_interface_pml import pml_damping, ring_mask
+    Ts = 300
+    dxp, dzp = pml_damping(sc.X, sc.Z, sc.PML)
+    sx, sz = sc.src_xz()
+    mx, mz = sc.rec_xz()
+    rz, rx = np.where(ring_mask(sc.X, sc.Z, sc.PML, np.where(sc.src_mask), 4))
+    src = sc.source[:1, :Ts]
+    args0 = (sc.c_true ** 2, np.ones(3), dxp, dzp, sx[:1], sz[:1], src, mx, mz)
+    obs = po.simulate(*args0, mode="f32")
+    t0 = time.perf_counter()
+    po.grad(sc.c_start ** 2, np.ones(3), dxp, dzp, sx[:1], sz[:1], src, mx, mz, rx, rz,
+            lambda s: mo.wasserstein_softplus(s, obs), mode="f64")
+    dt = time.perf_counter() - t0
+    v = 2 * sc.X * sc.Z * (Ts - 1) / dt / 1e9
+    return {"value": v, "unit": UNIT, "cores": po.num_threads(), "kind": "port",
+            "sample": f"FP64 oracle (oracle/pml_oracle.c, OpenMP) + numpy softplus-W2 misfit: 1 shot, "
+                      f"{sc.X}x{sc.Z}, first {Ts} of {sc.T} steps, forward + adjoint gradient, {dt:.1f} s"}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from otfwi_b200.batch import ShotBatch
+    sc = workload(args)
+    b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, prec_deriv=4,
+                  precision=args.precision, tile=args.tile)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+    c_true = torch.tensor(sc.c_true, dtype=torch.float32, device=dev)
+    c0 = torch.tensor(sc.c_start, dtype=torch.float32, device=dev)
+    obs = torch.empty((sc.n_src, sc.n_rec, sc.T), dtype=torch.float32, device=dev)
+    b.set_model(cquad=(c_true * c_true).contiguous())
+    b.forward(out=obs)
+    b.set_observed(obs)
+    b.set_model(cquad=(c0 * c0).contiguous())
+    grad = torch.empty((sc.Z, sc.X), dtype=torch.float32, device=dev)
+    mis = torch.empty(1, dtype=torch.float64, device=dev)
+
+    def step():
+        b.gradient(args.misfit, grad=grad, misfit_out=mis)
+        if world > 1:
+            with torch.cuda.stream(stream):
+                dist.all_reduce(grad)
+                dist.all_reduce(mis)
+
+    for _ in range(args.warmup):
+        step()
+    b.sync()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = 2 * sc.X * sc.Z * (sc.T - 1) * sc.n_src
+    value = cells * world / (ms / 1e3) / 1e9
+
+    # per-kernel live timing of the two step kernels (graphs of T-1 launches
+    # each), for the roofline of the dominant kernel
+    def time_graph(fn, reps=2):
+        fn()
+        b.sync()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(reps):
+            fn()
+        f1.record(stream)
+        f1.synchronize()
+        return f0.elapsed_time(f1) / reps / (sc.T - 1)
+
+    ms_fwd = time_graph(lambda: b._lib.otf_batch_forward_ring(b._h, None, 0))
+    b._lib.otf_batch_misfit(b._h, 2, None, 0)
+    ms_rev = time_graph(lambda: b._lib.otf_batch_reverse(b._h, None, 0, None, 1.0, 0))
+    peak, peak_kind = measured_peak()
+    per_launch_cells = sc.X * sc.Z * sc.n_src
+    ach_rev = BYTES_REV * per_launch_cells / (ms_rev / 1e3) / 1e9
+    ach_fwd = BYTES_FWD * per_launch_cells / (ms_fwd / 1e3) / 1e9
+    tr = profile_traffic()
+    roof = {"kernel": "k_reverse_step (adjoint + reconstruction + imaging condition, all shots)",
+            "bound": "hbm", "achieved": round(ach_rev, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(ach_rev / peak, 4), "peak_kind": peak_kind,
+            "traffic": (tr * per_launch_cells if tr else None),
+            "algorithmic_bytes_per_launch": BYTES_REV * per_launch_cells,
+            "launch_ms": round(ms_rev, 4),
+            "forward_kernel": {"achieved": round(ach_fwd, 1), "frac": round(ach_fwd / peak, 4),
+                               "launch_ms": round(ms_fwd, 4),
+                               "algorithmic_bytes_per_launch": BYTES_FWD * per_launch_cells},
+            "whole_step_frac": round(BYTES_STEP * sc.X * sc.Z * (sc.T - 1) * sc.n_src
+                                     / (ms / 1e3) / 1e9 / peak, 4)}
+
+    # end to end through the public API with host buffers: model and
+    # observed traces from pinned host memory, gradient and misfit back
+    h_cq = torch.tensor(sc.c_start.astype(np.float32) ** 2).pin_memory()
+    h_obs = obs.cpu().pin_memory()
+    h_grad = torch.empty((sc.Z, sc.X), dtype=torch.float32).pin_memory()
+    h_mis = torch.empty(1, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        b.set_model(cquad=h_cq.numpy())
+        b.set_observed(h_obs.numpy())
+        b._ok(b._lib.otf_batch_gradient(b._h, 2, __import__("ctypes").c_void_p(h_grad.data_ptr()),
+                                        __import__("ctypes").c_void_p(h_mis.data_ptr()), 0))
+        b.sync()
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    n_e2e = max(2, args.steps // 2)
+    for _ in range(n_e2e):
+        e2e_step()
+    g1.record(stream)
+    g1.synchronize()
+    ms_e2e = g0.elapsed_time(g1) / n_e2e
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = {"value": cells * world / (ms_e2e / 1e3) / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": int(h_cq.numel() * 4 + h_obs.numel() * 4),
+           "d2h_bytes_per_step": int(h_grad.numel() * 4 + 8), "ms_per_step": round(ms_e2e, 3)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded model, Ricker source; no external dataset)",
+                "config": config_block(args, sc, f"shots-per-rank, gradient all-reduce, {world} rank(s)"),
+                "roofline": roof, "e2e": e2e,
+                # per step: T-1 forward + T-1 reverse step kernels, misfit,
+                # misfit sum, adjoint running integral, shot mean
+                "gpu_launches": args.steps * (2 * (sc.T - 1) + 4),
+                "clocks": clk.summary(),
+                "misfit_value": float(mis.item())}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args, sc)
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's own CUDA library (oracle/_ref, compiled from
+    regression_PML_single.cu) driven as cuda_interface_pml.py drives it: one
+    cuda_grad_ext per shot with the host misfit callback (the reference's
+    wasserstein recipe, restated in oracle/misfit_oracle.py). Runs in this
+    process only; it must not share a CUDA context (the library resets the
+    device on init). Each step is a bounded sample of the FMC workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import ctypes
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import misfit_oracle as mo
+    from otfwi_b200.cuda_interface_pml import Cuda_interface_PML
+    path = os.path.join(ROOT, "oracle", "_ref", "cuda_regression_PML_single.so")
+    sc = workload(args)
+    cfg = config_block(args, sc, "reference per-shot loop, 1 GPU")
+    if not os.path.exists(path):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref library not built"}))
+        return
+    cp = Cuda_interface_PML(sc.X, sc.Z, sc.T, sc.PML, sc.c_true, sc.n_src, sc.src_mask, sc.n_rec,
+                            sc.rec_mask, sc.source, multishot=True, lib=path)
+    ns = args.ref_shots
+    obs = np.zeros((sc.n_src, sc.n_rec, sc.T), np.float32)
+    buf = np.zeros((sc.n_rec, sc.T), np.float32)
+    for s in range(ns):
+        cp._lib.cuda_simulate(0, s)
+        ctypes.memmove(buf.ctypes.data, cp.recptr[0], buf.nbytes)
+        obs[s] = buf
+    cp.init_regression(obs, mo.wasserstein, prec_deriv=4)
+    cp._set_c_quad(sc.c_start ** 2)
+
+    def step():
+        for s in range(ns):
+            cp.idx_source = s
+            mse = (ctypes.c_float * 1)(0.0)
+            cp._lib.cuda_grad_ext(mse, cp.adj_wrapper_ptr, s)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = 2 * sc.X * sc.Z * (sc.T - 1) * ns / dt / 1e9
+    sample = (f"reference CUDA library (regression_PML_single.cu built by oracle/Makefile) on the GPU, "
+              f"per-shot cuda_grad_ext with the host Wasserstein callback (reference recipe; the "
+              f"reference has no softplus variant): {ns} of {sc.n_src} shots per step")
+    print(json.dumps({"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": 1,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 2),
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                      "data": "synthetic", "config": cfg, "impl": "reference",
+                      "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": 1,
+                                       "kind": "reference", "sample": sample},
+                      "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

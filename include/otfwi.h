@@ -89,6 +89,64 @@ int otf_set_tile(int tile);
 /* Free every buffer of the drop-in state. */
 void otf_release(void);
 
+/* ---- Part 3: batched shots (additive) -----------------------------------
+ * Replaces the per-shot loops of Cuda_interface_PML.simulate / calc_grad
+ * (cuda_interface_pml.py:185-236) and the host misfit callback
+ * (cuda_interface_pml.py:238-249 -> adjoint_functions.py): every shot of a
+ * shot table advances in the same launches, the misfit and adjoint sources
+ * are computed on the device, and the whole gradient is one CUDA graph.
+ * Pointers flagged on_device are device pointers (e.g. torch tensors on the
+ * same device), otherwise host pointers. Calls are asynchronous on the
+ * handle's stream (otf_batch_stream); otf_batch_sync waits. Return 0 on
+ * success, -1 on failure (message in otf_last_error). */
+typedef struct otf_batch otf_batch;
+
+/* Same inputs as init_memory_sim + init_memory_reg: grid, constvec, damping
+ * [Z*X], sources with waveforms [n_src*T], receivers, boundary ring; room for
+ * max_shots shots; precision 0 faithful / 1 fast; tile shape index. */
+otf_batch *otf_batch_create(int X, int Z, int T, const float *constvec, const float *d_x,
+                            const float *d_z, int n_src, const int *src_x, const int *src_z,
+                            const float *source, int n_rec, const int *rec_x, const int *rec_z,
+                            int n_ring, const int *ring_x, const int *ring_z, int max_shots,
+                            int precision, int tile);
+void otf_batch_destroy(otf_batch *b);
+/* Shot s fires sources srcs[ptr[s] .. ptr[s+1]) (full-matrix capture: ptr =
+ * 0..n, srcs = 0..n-1). The reference's idx_source == -1 is one shot firing
+ * every source. */
+int otf_batch_set_shots(otf_batch *b, int n_shots, const int *ptr, const int *srcs);
+int otf_batch_set_model(otf_batch *b, const float *cquad, int on_device);       /* [Z*X] */
+int otf_batch_set_observed(otf_batch *b, const float *obs, int on_device);      /* [n_shots*n_rec*T] */
+int otf_batch_set_precision(otf_batch *b, int precision);
+int otf_batch_set_tile(otf_batch *b, int tile);
+/* Forward modelling of every shot; traces [n_shots][n_rec][T] (NULL: keep). */
+int otf_batch_forward(otf_batch *b, float *traces, int on_device);
+/* Forward with boundary-ring recording (gradient phase 1). */
+int otf_batch_forward_ring(otf_batch *b, float *traces, int on_device);
+/* Full gradient: forward, device misfit (0 = L2, 1 = Wasserstein as
+ * adjoint_functions.wasserstein, 2 = Wasserstein on softplus-normalised
+ * traces), reverse phase; grad [Z*X] = mean over shots of the per-shot
+ * gradients, *misfit = sum over every trace (both optional). */
+int otf_batch_gradient(otf_batch *b, int misfit_kind, float *grad, double *misfit, int on_device);
+/* Device misfit of the last forward traces against the observed traces:
+ * per-trace misfits [n_shots*n_rec] (optional) and the adjoint sources. */
+int otf_batch_misfit(otf_batch *b, int misfit_kind, double *per_trace, int on_device);
+int otf_batch_adjoint(otf_batch *b, float *adj, int on_device);  /* copy out the adjoint sources */
+/* Reverse phase after otf_batch_forward_ring, with adjoint sources adj
+ * [n_shots][n_rec][T] (NULL: those of otf_batch_misfit); grad [Z*X] =
+ * scale * sum over shots. */
+int otf_batch_reverse(otf_batch *b, const float *adj, int on_device, float *grad, float scale,
+                      int grad_on_device);
+int otf_batch_shot_grad(otf_batch *b, int shot, float *grad, int on_device); /* one shot's [Z*X] */
+int otf_batch_sync(otf_batch *b);
+void *otf_batch_stream(otf_batch *b);
+
+/* Stand-alone device misfit over n_traces traces [n_traces][T] (device
+ * pointers, misfit [n_traces] FP64) with caller-owned scratch of at least
+ * otf_misfit_scratch_bytes(kind, n_traces, T) bytes, on a cudaStream_t. */
+long long otf_misfit_scratch_bytes(int kind, int n_traces, int T);
+int otf_misfit(int kind, const float *sim, const float *obs, float *adj, double *misfit,
+               int n_traces, int T, void *scratch, long long scratch_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

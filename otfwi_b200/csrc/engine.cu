@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 #include "engine.h"
+#include "misfit.h"
 
 namespace otf {
 
@@ -80,8 +81,9 @@ __global__ void k_prep_q(const float *__restrict__ cq, float *__restrict__ qf,
 }
 
 // Sum of the padded per-shot gradients into an unpadded [Z*X] array, in shot
-// order (the wrapper's grad_acc += grad loop, cuda_interface_pml.py:225-235),
-// then scaled.
+// order, then either divided by the shot count in FP32 (the wrapper's
+// grad_acc += grad; grad_acc / n_source, cuda_interface_pml.py:225-235) when
+// scale == 0, or multiplied by scale.
 __global__ void k_grad_sum(const float *__restrict__ g, float *__restrict__ out, Layout L,
                            int n_shots, int64_t stride, float scale)
 {
@@ -93,7 +95,8 @@ __global__ void k_grad_sum(const float *__restrict__ g, float *__restrict__ out,
     float acc = 0.f;
     for (int s = 0; s < n_shots; s++)
         acc = __fadd_rn(acc, g[o + stride * s]);
-    out[i] = scale == 1.f ? acc : __fmul_rn(acc, scale);
+    out[i] = scale == 0.f ? __fdiv_rn(acc, (float)n_shots)
+                          : (scale == 1.f ? acc : __fmul_rn(acc, scale));
 }
 
 // ------------------------------------------------------- kernel dispatch
@@ -176,6 +179,11 @@ void Engine::drop_graphs()
     if (g_rev_)
         cudaGraphExecDestroy(g_rev_);
     g_fwd_ = g_fwd_ring_ = g_rev_ = nullptr;
+    for (auto &g : g_grad_) {
+        if (g)
+            cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
     graph_shots_ = -1;
 }
 
@@ -185,12 +193,19 @@ void Engine::free_all()
     if (qr_ == qf_)
         qr_ = nullptr;  // aliased when dt == dx == 1: freed once, as qf_
     float **fl[] = {&qf_, &qr_, &dampx_, &dampz_, &dampx2_, &dampz2_, &grad_, &rec_, &ring_,
-                    &src_, &tab_src_, &adj_, &tab_adj_};
+                    &src_, &tab_src_, &adj_, &tab_adj_, &obs_};
     for (float **p : fl) {
         if (*p)
             cudaFree(*p);
         *p = nullptr;
     }
+    if (mis_)
+        cudaFree(mis_);
+    mis_ = nullptr;
+    if (mscratch_)
+        cudaFree(mscratch_);
+    mscratch_ = nullptr;
+    mscratch_bytes_ = 0;
     for (auto &a : fld_)
         for (auto &b : a)
             for (auto &c : b) {
@@ -377,7 +392,7 @@ int Engine::set_receivers(int n, const int *x, const int *z)
     rec_x_.assign(x, x + n);
     rec_z_.assign(z, z + n);
     n_rec_ = n;
-    float **bufs[] = {&rec_, &adj_, &tab_adj_};
+    float **bufs[] = {&rec_, &adj_, &tab_adj_, &obs_};
     for (float **b : bufs) {
         if (*b)
             cudaFree(*b);
@@ -388,6 +403,14 @@ int Engine::set_receivers(int n, const int *x, const int *z)
         OTF_CUDA(cudaMalloc(b, sz));
         OTF_CUDA(cudaMemset(*b, 0, sz));
     }
+    if (mis_)
+        cudaFree(mis_);
+    mis_ = nullptr;
+    OTF_CUDA(cudaMalloc(&mis_, sizeof(double) * ((size_t)std::max(n, 1) * cfg_.max_shots + 1)));
+    if (mscratch_)
+        cudaFree(mscratch_);
+    mscratch_ = nullptr;
+    mscratch_bytes_ = 0;
     tables_dirty_ = true;
     drop_graphs();
     return 0;
@@ -634,7 +657,9 @@ static dim3 step_grid(const EngineConfig &c, int n_shots)
     return dim3((unsigned)(ntx * ntz), (unsigned)n_shots, 1);
 }
 
-int Engine::capture_forward(bool with_ring, cudaGraphExec_t *out)
+// Emit (into the stream, normally under capture) the forward time loop:
+// zero the fields, then one fused launch per step.
+int Engine::emit_forward(bool with_ring)
 {
     StepParams p = base_params();
     p.q0 = qf_;
@@ -646,32 +671,29 @@ int Engine::capture_forward(bool with_ring, cudaGraphExec_t *out)
     p.inj_tab = tab_src_;
     const dim3 grid = step_grid(cfg_, n_shots_);
     const size_t fbytes = sizeof(float) * (size_t)L_.slot * n_shots_;
-    cudaGraph_t g = nullptr;
-    OTF_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-    int rc = 0;
-    for (int f = 0; f < 4 && !rc; f++)
-        for (int s = 0; s < 2 && !rc; s++)
-            if (cudaMemsetAsync(fld_[0][f][s], 0, fbytes, st_) != cudaSuccess)
-                rc = -1;
-    for (int t = 1; t < cfg_.T && !rc; t++) {
+    for (int f = 0; f < 4; f++)
+        for (int s = 0; s < 2; s++)
+            OTF_CUDA(cudaMemsetAsync(fld_[0][f][s], 0, fbytes, st_));
+    for (int t = 1; t < cfg_.T; t++) {
         const int i = (t - 1) & 1, o = t & 1;
         p.t = t;
         p.f0 = Fields{fld_[0][0][i], fld_[0][1][i], fld_[0][2][i], fld_[0][3][i],
                       fld_[0][0][o], fld_[0][1][o], fld_[0][2][o], fld_[0][3][o]};
-        rc = launch_forward_step(p, with_ring, grid);
+        if (launch_forward_step(p, with_ring, grid))
+            return -1;
     }
-    const cudaError_t ec = cudaStreamEndCapture(st_, &g);
-    if (rc)
-        return rc;
-    OTF_CUDA(ec);
-    const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
-    cudaGraphDestroy(g);
-    OTF_CUDA(ei);
     return 0;
 }
 
-int Engine::capture_reverse(cudaGraphExec_t *out)
+// Emit the reverse time loop: running integral of the time-flipped adjoint
+// source, zeroed adjoint fields and gradient, one fused launch per step.
+int Engine::emit_reverse()
 {
+    const int rows = n_rec_ * n_shots_;
+    if (rows > 0) {
+        k_prefix_rows<<<(rows + 127) / 128, 128, 0, st_>>>(adj_, tab_adj_, rows, cfg_.T, 1);
+        OTF_CUDA(cudaGetLastError());
+    }
     StepParams p = base_params();
     p.q0 = qr_;
     p.q1 = qf_;
@@ -683,16 +705,11 @@ int Engine::capture_reverse(cudaGraphExec_t *out)
     const dim3 grid = step_grid(cfg_, n_shots_);
     const size_t fbytes = sizeof(float) * (size_t)L_.slot * n_shots_;
     const int T = cfg_.T;
-    cudaGraph_t g = nullptr;
-    OTF_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-    int rc = 0;
-    for (int f = 0; f < 4 && !rc; f++)
-        for (int s = 0; s < 2 && !rc; s++)
-            if (cudaMemsetAsync(fld_[1][f][s], 0, fbytes, st_) != cudaSuccess)
-                rc = -1;
-    if (!rc && cudaMemsetAsync(grad_, 0, fbytes, st_) != cudaSuccess)
-        rc = -1;
-    for (int t = 1; t < T && !rc; t++) {
+    for (int f = 0; f < 4; f++)
+        for (int s = 0; s < 2; s++)
+            OTF_CUDA(cudaMemsetAsync(fld_[1][f][s], 0, fbytes, st_));
+    OTF_CUDA(cudaMemsetAsync(grad_, 0, fbytes, st_));
+    for (int t = 1; t < T; t++) {
         // reconstruction starts from P(T-1) (slot (T-1)%2) and A(T-2)
         // (slot (T-2)%2) (regression_PML_single.cu:787-790) and ping-pongs
         const int pi = (T + t) & 1, po = (T + t + 1) & 1;
@@ -703,11 +720,25 @@ int Engine::capture_reverse(cudaGraphExec_t *out)
                       fld_[0][0][po], fld_[0][1][po], fld_[0][2][ao], fld_[0][3][ao]};
         p.f1 = Fields{fld_[1][0][i], fld_[1][1][i], fld_[1][2][i], fld_[1][3][i],
                       fld_[1][0][o], fld_[1][1][o], fld_[1][2][o], fld_[1][3][o]};
-        rc = launch_reverse_step(p, grid);
+        if (launch_reverse_step(p, grid))
+            return -1;
     }
+    return 0;
+}
+
+// Capture whatever `emit` puts on the stream into an instantiated graph.
+template <class Emit>
+int Engine::capture(cudaGraphExec_t *out, Emit emit)
+{
+    cudaGraph_t g = nullptr;
+    OTF_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    const int rc = emit();
     const cudaError_t ec = cudaStreamEndCapture(st_, &g);
-    if (rc)
+    if (rc) {
+        if (g)
+            cudaGraphDestroy(g);
         return rc;
+    }
     OTF_CUDA(ec);
     const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
@@ -715,14 +746,21 @@ int Engine::capture_reverse(cudaGraphExec_t *out)
     return 0;
 }
 
-int Engine::forward(bool with_ring)
+int Engine::prepare()
 {
     OTF_CHECK(ready_, 2, "engine not initialised");
     OTF_CHECK(!shot_ptr_.empty(), 2, "no shots configured");
     if (tables_dirty_ && build_tables())
         return -1;
+    return 0;
+}
+
+int Engine::forward(bool with_ring)
+{
+    if (prepare())
+        return -1;
     cudaGraphExec_t *g = with_ring ? &g_fwd_ring_ : &g_fwd_;
-    if (!*g && capture_forward(with_ring, g))
+    if (!*g && capture(g, [&] { return emit_forward(with_ring); }))
         return -1;
     OTF_CUDA(cudaGraphLaunch(*g, st_));
     return 0;
@@ -730,17 +768,44 @@ int Engine::forward(bool with_ring)
 
 int Engine::reverse()
 {
-    OTF_CHECK(ready_, 2, "engine not initialised");
-    if (tables_dirty_ && build_tables())
+    if (prepare())
         return -1;
-    const int rows = n_rec_ * n_shots_;
-    if (rows > 0) {
-        k_prefix_rows<<<(rows + 127) / 128, 128, 0, st_>>>(adj_, tab_adj_, rows, cfg_.T, 1);
-        OTF_CUDA(cudaGetLastError());
-    }
-    if (!g_rev_ && capture_reverse(&g_rev_))
+    if (!g_rev_ && capture(&g_rev_, [&] { return emit_reverse(); }))
         return -1;
     OTF_CUDA(cudaGraphLaunch(g_rev_, st_));
+    return 0;
+}
+
+// The whole multi-shot gradient as one graph: forward with ring recording,
+// device misfit and adjoint sources, reverse phase, and the shot mean of the
+// gradients into grad_mean_dev() / the misfit total into misfit_total_dev().
+int Engine::gradient(int kind)
+{
+    if (prepare())
+        return -1;
+    OTF_CHECK(kind >= 0 && kind < 3, 1, "unknown misfit kind");
+    if (!gsum_) {
+        OTF_CUDA(cudaMalloc(&gsum_, sizeof(float) * (size_t)cfg_.X * cfg_.Z));
+        OTF_CUDA(cudaMalloc(&tot_, sizeof(double)));
+    }
+    // the misfit scratch must exist before capture (no allocation inside a graph)
+    const int64_t need = misfit_scratch_per_trace(kind, cfg_.T) * n_shots_ * n_rec_;
+    if (need > mscratch_bytes_) {
+        drop_graphs();
+        if (mscratch_)
+            OTF_CUDA(cudaFree(mscratch_));
+        mscratch_ = nullptr;
+        OTF_CUDA(cudaMalloc(&mscratch_, (size_t)need));
+        mscratch_bytes_ = need;
+    }
+    if (!g_grad_[kind] && capture(&g_grad_[kind], [&] {
+            if (emit_forward(true) || misfit(kind, tot_) || emit_reverse() ||
+                grad_sum(gsum_, 0.0f))
+                return -1;
+            return 0;
+        }))
+        return -1;
+    OTF_CUDA(cudaGraphLaunch(g_grad_[kind], st_));
     return 0;
 }
 
@@ -770,6 +835,45 @@ int Engine::grad_sum(float *dst, float scale)
 int Engine::sync()
 {
     OTF_CUDA(cudaStreamSynchronize(st_));
+    return 0;
+}
+
+int Engine::set_observed(const float *obs, cudaMemcpyKind kind)
+{
+    OTF_CHECK(ready_ && obs_, 2, "receivers not configured");
+    const size_t n = (size_t)n_shots_ * n_rec_ * cfg_.T;
+    OTF_CUDA(cudaMemcpyAsync(obs_, obs, sizeof(float) * n, kind, st_));
+    return 0;
+}
+
+// Sum of the per-trace misfits in trace order (FP64), one thread.
+__global__ void k_sum_misfit(const double *__restrict__ m, int n, double *__restrict__ out)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; i++)
+        s += m[i];
+    *out = s;
+}
+
+int Engine::misfit(int kind, double *total_dev)
+{
+    OTF_CHECK(ready_ && obs_, 2, "receivers not configured");
+    const int n = n_shots_ * n_rec_;
+    const int64_t need = misfit_scratch_per_trace(kind, cfg_.T) * n;
+    if (need > mscratch_bytes_) {
+        if (mscratch_)
+            OTF_CUDA(cudaFree(mscratch_));
+        mscratch_ = nullptr;
+        mscratch_bytes_ = 0;
+        OTF_CUDA(cudaMalloc(&mscratch_, (size_t)need));
+        mscratch_bytes_ = need;
+    }
+    if (launch_misfit(kind, rec_, obs_, adj_, mis_, n, cfg_.T, mscratch_, mscratch_bytes_, st_))
+        return -1;
+    if (total_dev) {
+        k_sum_misfit<<<1, 1, 0, st_>>>(mis_, n, total_dev);
+        OTF_CUDA(cudaGetLastError());
+    }
     return 0;
 }
 

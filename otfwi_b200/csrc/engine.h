@@ -54,10 +54,22 @@ class Engine {
     // Copies of results.
     int copy_traces(float *dst, int shot0, int n, cudaMemcpyKind kind);
     int copy_grad_shot(int shot, float *dst, cudaMemcpyKind kind);  // unpadded [Z*X]
-    int grad_sum(float *dst_dev_unpadded, float scale);             // sum over shots * scale
+    // sum over shots * scale; scale == 0: sum / n_shots (FP32 division)
+    int grad_sum(float *dst_dev_unpadded, float scale);
+
+    // Observed traces [n_shots][n_rec][T] and the device misfit: fills
+    // adj_dev() from rec_dev() vs observed, per-trace misfits into
+    // misfit_dev() [n_shots*n_rec] and their sum into *total_dev (device).
+    int set_observed(const float *obs, cudaMemcpyKind kind);
+    int misfit(int kind, double *total_dev);
+    // forward + misfit + reverse + shot mean, replayed as one CUDA graph
+    int gradient(int kind);
+    float *grad_mean_dev() { return gsum_; }
+    double *misfit_total_dev() { return tot_; }
 
     float *rec_dev() { return rec_; }
     float *adj_dev() { return adj_; }
+    double *misfit_dev() { return mis_; }
     cudaStream_t stream() const { return st_; }
     int n_shots() const { return n_shots_; }
     int n_rec() const { return n_rec_; }
@@ -69,8 +81,11 @@ class Engine {
 
   private:
     int build_tables();
-    int capture_forward(bool with_ring, cudaGraphExec_t *out);
-    int capture_reverse(cudaGraphExec_t *out);
+    int prepare();
+    int emit_forward(bool with_ring);
+    int emit_reverse();
+    template <class Emit>
+    int capture(cudaGraphExec_t *out, Emit emit);
     int launch_forward_step(const StepParams &p, bool with_ring, dim3 grid);
     int launch_reverse_step(const StepParams &p, dim3 grid);
     void drop_graphs();
@@ -97,6 +112,10 @@ class Engine {
     float *ring_ = nullptr;     // [max_shots][T][n_ring]
     float *src_ = nullptr, *tab_src_ = nullptr;  // [n_src][T]
     float *adj_ = nullptr, *tab_adj_ = nullptr;  // [max_shots][n_rec][T]
+    float *obs_ = nullptr;                       // [max_shots][n_rec][T]
+    double *mis_ = nullptr;                      // [max_shots*n_rec]
+    void *mscratch_ = nullptr;                   // misfit CDF scratch
+    int64_t mscratch_bytes_ = 0;
     int *inj_src_ = nullptr;   // CSR: ptr[max_shots+1] | x | z | row
     int *inj_adj_ = nullptr;
     int *tabs_ = nullptr;      // per-tile receiver / ring tables
@@ -108,6 +127,9 @@ class Engine {
     int *inj_adj_ptr_ = nullptr, *inj_adj_x_ = nullptr, *inj_adj_z_ = nullptr, *inj_adj_row_ = nullptr;
 
     cudaGraphExec_t g_fwd_ = nullptr, g_fwd_ring_ = nullptr, g_rev_ = nullptr;
+    cudaGraphExec_t g_grad_[3] = {nullptr, nullptr, nullptr};  // per misfit kind
+    float *gsum_ = nullptr;  // [Z*X] shot-mean gradient of the last gradient()
+    double *tot_ = nullptr;  // misfit total of the last gradient()
     int graph_shots_ = -1;
     bool tables_dirty_ = true;
 };
