@@ -147,6 +147,19 @@ long long otf_misfit_scratch_bytes(int kind, int n_traces, int T);
 int otf_misfit(int kind, const float *sim, const float *obs, float *adj, double *misfit,
                int n_traces, int T, void *scratch, long long scratch_bytes, void *stream);
 
+/* Same as otf_misfit, but allocates nothing: no counterpart in the
+ * reference. For callers that cannot allocate device memory when they need
+ * a misfit -- their GPU memory is already reserved by another allocator, or
+ * they cannot afford cudaMalloc/cudaFree, which may synchronise the device.
+ * The scratch is a 16 MiB array built into the library (held on every GPU
+ * that loads it until exit); n_traces * otf_misfit_scratch_bytes(kind, 1, T)
+ * above 16 MiB is rejected with an error (returns -1). The first call on a
+ * device looks the array's device address up: make it before any stream
+ * capture. All calls share the array: calls that may overlap on the GPU race,
+ * so order them on one stream. Inputs and outputs are caller device memory. */
+int otf_misfit_noalloc(int kind, const float *sim, const float *obs, float *adj, double *misfit,
+                       int n_traces, int T, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -419,3 +419,71 @@ int launch_misfit(int kind, const float *sim, const float *obs, float *adj, doub
 }
 
 }  // namespace otf
+
+// ---------------------------------------------------------------------------
+// Misfit without any device allocation.
+//
+// Some callers cannot allocate device memory at the moment they need a
+// misfit: a host whose GPU memory is already fully reserved by another
+// allocator (a framework that preallocates most of the device, so cudaMalloc
+// fails), or a time-critical loop that must not pay for cudaMalloc/cudaFree,
+// which can synchronise the whole device and stall other streams. For them
+// the CDF scratch of the misfit kernel lives in the fixed array below,
+// compiled into the library: every GPU that loads the library holds these
+// 16 MiB until the process exits.
+//
+// Host code cannot use the array's name as a device address (in host code it
+// names a host-side stand-in), so its device address is looked up once per
+// device, with that device current, by cudaGetSymbolAddress. That set-up is
+// done by the first otf_misfit_noalloc call on each device; make that first
+// call before any stream capture. All calls share the one array and it keeps
+// whatever the last call left there; the kernel writes every scratch element
+// it reads, so nothing has to be cleared between calls. Calls whose kernels
+// may run at the same time on the GPU (different streams without ordering
+// between them) race on the array: serialise them.
+#include <mutex>
+#include <string>
+
+namespace {
+constexpr long long kNoAllocScratchBytes = 16ll << 20;
+__device__ __align__(256) char g_noalloc_misfit_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kMaxDevices] = {};
+
+// device address of the scratch array on the current device (looked up once)
+int noalloc_scratch(void **out)
+{
+    int dev = -1;
+    OTF_CUDA(cudaGetDevice(&dev));
+    OTF_CHECK(dev >= 0 && dev < kMaxDevices, 1, "otf_misfit_noalloc: device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        OTF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_misfit_scratch));
+        OTF_CHECK(p != nullptr, 1, "otf_misfit_noalloc: scratch address lookup returned null");
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return 0;
+}
+}  // namespace
+
+extern "C" int otf_misfit_noalloc(int kind, const float *sim, const float *obs, float *adj,
+                                  double *misfit, int n_traces, int T, void *stream)
+{
+    OTF_CHECK(T >= 2, 1, "otf_misfit_noalloc: T must be at least 2");
+    OTF_CHECK(n_traces >= 0, 1, "otf_misfit_noalloc: negative trace count");
+    const long long need = (long long)otf::misfit_scratch_per_trace(kind, T) * n_traces;
+    OTF_CHECK(need <= kNoAllocScratchBytes, 1,
+              "otf_misfit_noalloc: " + std::to_string(n_traces) + " traces of " + std::to_string(T) +
+                  " samples need " + std::to_string(need) +
+                  " bytes of scratch, more than the built-in 16 MiB; split the traces over several "
+                  "calls or use otf_misfit with your own scratch");
+    void *scratch = nullptr;
+    if (noalloc_scratch(&scratch))
+        return -1;
+    return otf::launch_misfit(kind, sim, obs, adj, misfit, n_traces, T, scratch,
+                              kNoAllocScratchBytes, (cudaStream_t)stream);
+}
