@@ -118,6 +118,10 @@ int otf_batch_set_model(otf_batch *b, const float *cquad, int on_device);       
 int otf_batch_set_observed(otf_batch *b, const float *obs, int on_device);      /* [n_shots*n_rec*T] */
 int otf_batch_set_precision(otf_batch *b, int precision);
 int otf_batch_set_tile(otf_batch *b, int tile);
+/* 0: one tile per CTA per step; 1 (default): persistent CTAs with TMA
+ * double-buffered halo tiles (tile shapes 0, 1 and 4; others use 0).
+ * Both give bit-identical results. */
+int otf_batch_set_kernel(otf_batch *b, int variant);
 /* Forward modelling of every shot; traces [n_shots][n_rec][T] (NULL: keep). */
 int otf_batch_forward(otf_batch *b, float *traces, int on_device);
 /* Forward with boundary-ring recording (gradient phase 1). */

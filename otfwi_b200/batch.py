@@ -36,6 +36,7 @@ def _declare(lib):
         "otf_batch_set_observed": [c_void_p, c_void_p, c_int],
         "otf_batch_set_precision": [c_void_p, c_int],
         "otf_batch_set_tile": [c_void_p, c_int],
+        "otf_batch_set_kernel": [c_void_p, c_int],
         "otf_batch_forward": [c_void_p, c_void_p, c_int],
         "otf_batch_forward_ring": [c_void_p, c_void_p, c_int],
         "otf_batch_gradient": [c_void_p, c_int, c_void_p, c_void_p, c_int],
@@ -95,7 +96,7 @@ class ShotBatch:
 
     def __init__(self, X, Z, T, PML_size, src_mask, rec_mask, source, prec_deriv=4, shots=None,
                  max_shots=None, precision=0, tile=0, constvec=(1.0, 1.0, 1.0), d_x=None, d_z=None,
-                 lib=None):
+                 kernel=1, lib=None):
         self._lib = _declare(_lib.load(lib))
         self.X, self.Z, self.T, self.PML = X, Z, T, PML_size
         pz, px = np.where(src_mask)
@@ -118,6 +119,7 @@ class ShotBatch:
             _lib.check(self._lib)
             raise _lib.OtfwiError("otf_batch_create failed")
         self._h = c_void_p(h)
+        self.set_kernel(kernel)
         self.set_shots(ptr, srcs)
 
     def _ok(self, rc):
@@ -166,6 +168,10 @@ class ShotBatch:
 
     def set_tile(self, tile):
         self._ok(self._lib.otf_batch_set_tile(self._h, tile))
+
+    def set_kernel(self, variant):
+        """0: one tile per CTA per step; 1: persistent TMA-pipelined CTAs."""
+        self._ok(self._lib.otf_batch_set_kernel(self._h, variant))
 
     def sync(self):
         self._ok(self._lib.otf_batch_sync(self._h))

@@ -5,12 +5,13 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <cudaTypedefs.h>
 #include "engine.h"
 #include "misfit.h"
 
 namespace otf {
 
-const TileShape kTileShapes[kNumTileShapes] = {{56, 56}, {120, 24}, {120, 56}, {248, 24}};
+const TileShape kTileShapes[kNumTileShapes] = {{56, 56}, {120, 24}, {120, 56}, {248, 24}, {56, 24}};
 
 // ---------------------------------------------------------------- errors
 static thread_local int g_status = 0;
@@ -102,16 +103,23 @@ __global__ void k_grad_sum(const float *__restrict__ g, float *__restrict__ out,
 // ------------------------------------------------------- kernel dispatch
 
 struct KernelSet {
+    // v1: one tile per CTA
     void (*fwd)(const StepParams);
     void (*fwd_ring)(const StepParams);
     void (*rev)(const StepParams);
     size_t smem;
+    // v2: persistent, TMA-pipelined (null when the shape does not fit)
+    void (*fwd_tma)(const TmaParams);
+    void (*fwd_ring_tma)(const TmaParams);
+    void (*rev_tma)(const TmaParams);
+    size_t smem_fwd_tma, smem_rev_tma;
+    int grid_fwd_tma, grid_rev_tma;  // persistent grid sizes (set with the attributes)
 };
 
 template <int TX, int TZ, class Prec, bool SEP>
 static KernelSet make_set()
 {
-    KernelSet k;
+    KernelSet k{};
     k.fwd = k_forward_step<TX, TZ, Prec, SEP, false>;
     k.fwd_ring = k_forward_step<TX, TZ, Prec, SEP, true>;
     k.rev = k_reverse_step<TX, TZ, Prec, SEP>;
@@ -119,13 +127,16 @@ static KernelSet make_set()
     return k;
 }
 
-template <int TX, int TZ>
-static void fill_shape(KernelSet (&s)[2][2])
+template <int TX, int TZ, class Prec, bool SEP, int MINB>
+static KernelSet make_set_tma()
 {
-    s[kFaithful][1] = make_set<TX, TZ, Faithful, true>();
-    s[kFast][1] = make_set<TX, TZ, Fast, true>();
-    s[kFaithful][0] = KernelSet{nullptr, nullptr, nullptr, 0};
-    s[kFast][0] = KernelSet{nullptr, nullptr, nullptr, 0};
+    KernelSet k = make_set<TX, TZ, Prec, SEP>();
+    k.fwd_tma = k_forward_tma<TX, TZ, Prec, SEP, false, MINB>;
+    k.fwd_ring_tma = k_forward_tma<TX, TZ, Prec, SEP, true, MINB>;
+    k.rev_tma = k_reverse_tma<TX, TZ, Prec, SEP, MINB>;
+    k.smem_fwd_tma = TmaGeom<TX, TZ>::FWD_BYTES;
+    k.smem_rev_tma = TmaGeom<TX, TZ>::REV_BYTES;
+    return k;
 }
 
 struct KernelTable {
@@ -133,18 +144,28 @@ struct KernelTable {
     bool attrs_set = false;
     KernelTable()
     {
-        fill_shape<56, 56>(s[0]);
-        fill_shape<120, 24>(s[1]);
-        fill_shape<120, 56>(s[2]);
-        fill_shape<248, 24>(s[3]);
+        memset(s, 0, sizeof(s));
+        s[0][kFaithful][1] = make_set_tma<56, 56, Faithful, true, 1>();
+        s[0][kFast][1] = make_set_tma<56, 56, Fast, true, 1>();
+        s[1][kFaithful][1] = make_set_tma<120, 24, Faithful, true, 1>();
+        s[1][kFast][1] = make_set_tma<120, 24, Fast, true, 1>();
+        s[2][kFaithful][1] = make_set<120, 56, Faithful, true>();
+        s[2][kFast][1] = make_set<120, 56, Fast, true>();
+        s[3][kFaithful][1] = make_set<248, 24, Faithful, true>();
+        s[3][kFast][1] = make_set<248, 24, Fast, true>();
+        s[4][kFaithful][1] = make_set_tma<56, 24, Faithful, true, 2>();
+        s[4][kFast][1] = make_set_tma<56, 24, Fast, true, 2>();
         // general (non-separable) damping: compiled for the first shape only
-        s[0][kFaithful][0] = make_set<56, 56, Faithful, false>();
-        s[0][kFast][0] = make_set<56, 56, Fast, false>();
+        s[0][kFaithful][0] = make_set_tma<56, 56, Faithful, false, 1>();
+        s[0][kFast][0] = make_set_tma<56, 56, Fast, false, 1>();
     }
     int set_attrs()
     {
         if (attrs_set)
             return 0;
+        int dev = 0, nsm = 0;
+        OTF_CUDA(cudaGetDevice(&dev));
+        OTF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         for (auto &a : s)
             for (auto &b : a)
                 for (auto &k : b) {
@@ -155,6 +176,24 @@ struct KernelTable {
                         OTF_CUDA(cudaFuncSetAttribute((const void *)f,
                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                       (int)k.smem));
+                    if (!k.fwd_tma)
+                        continue;
+                    int nb = 0;
+                    void (*ft[2])(const TmaParams) = {k.fwd_tma, k.fwd_ring_tma};
+                    for (auto f : ft) {
+                        OTF_CUDA(cudaFuncSetAttribute((const void *)f,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)k.smem_fwd_tma));
+                        OTF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, NT, k.smem_fwd_tma));
+                        OTF_CHECK(nb >= 1, 4, "persistent forward kernel does not fit on an SM");
+                        k.grid_fwd_tma = nb * nsm;
+                    }
+                    OTF_CUDA(cudaFuncSetAttribute((const void *)k.rev_tma,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)k.smem_rev_tma));
+                    OTF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.rev_tma, NT, k.smem_rev_tma));
+                    OTF_CHECK(nb >= 1, 4, "persistent reverse kernel does not fit on an SM");
+                    k.grid_rev_tma = nb * nsm;
                 }
         attrs_set = true;
         return 0;
@@ -164,6 +203,28 @@ static KernelTable &ktable()
 {
     static KernelTable t;
     return t;
+}
+
+// Tiled tensor map over a padded [shots][rows][pitch] float array.
+static int encode_map(CUtensorMap *m, const float *base, const Layout &L, int shots, int bx, int bz)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        OTF_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        OTF_CHECK(q == cudaDriverEntryPointSuccess && p, 4, "cuTensorMapEncodeTiled is unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    cuuint64_t dims[3] = {(cuuint64_t)L.pitch, (cuuint64_t)L.rows, (cuuint64_t)shots};
+    cuuint64_t strides[2] = {(cuuint64_t)L.pitch * sizeof(float), (cuuint64_t)L.slot * sizeof(float)};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)bz, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    OTF_CHECK(r == CUDA_SUCCESS, 4, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+    return 0;
 }
 
 // ----------------------------------------------------------------- Engine
@@ -219,6 +280,12 @@ void Engine::free_all()
             cudaFree(*p);
         *p = nullptr;
     }
+    if (derr_)
+        cudaFree(derr_);
+    derr_ = nullptr;
+    delete tmap_;
+    tmap_ = nullptr;
+    maps_dirty_ = true;
     if (st_)
         cudaStreamDestroy(st_);
     st_ = nullptr;
@@ -297,6 +364,9 @@ int Engine::init(const EngineConfig &cfg, const float *d_x, const float *d_z)
             }
     OTF_CUDA(cudaMalloc(&grad_, fsz));
     OTF_CUDA(cudaMemset(grad_, 0, fsz));
+    OTF_CUDA(cudaMalloc(&derr_, sizeof(int)));
+    OTF_CUDA(cudaMemset(derr_, 0, sizeof(int)));
+    maps_dirty_ = true;
     ready_ = true;
     return 0;
 }
@@ -319,6 +389,7 @@ int Engine::set_tile(int tile)
     if (tile != cfg_.tile) {
         cfg_.tile = tile;
         tables_dirty_ = true;
+        maps_dirty_ = true;
         drop_graphs();
     }
     return 0;
@@ -633,20 +704,95 @@ StepParams Engine::base_params() const
     return p;
 }
 
-int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid)
+bool use_tma(const KernelSet &k, int variant) { return variant == 1 && k.fwd_tma != nullptr; }
+
+int Engine::variant_in_use() const
+{
+    return use_tma(ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0], variant_) ? 1 : 0;
+}
+
+// One forward step launch. pin / ain: slots holding P(t-1) / A(t-1).
+int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, int pin, int ain)
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
+    if (use_tma(k, variant_)) {
+        TmaParams P = *tmap_;
+        P.p = p;
+        P.s0_p_in = pin;
+        P.s0_a_in = ain;
+        P.s1_in = 0;
+        P.n_tiles = (int)grid.x;
+        P.n_items = (int)(grid.x * grid.y);
+        P.err = derr_;
+        void *args[] = {(void *)&P};
+        OTF_CUDA(cudaLaunchKernel((const void *)(with_ring ? k.fwd_ring_tma : k.fwd_tma),
+                                  dim3(std::min(k.grid_fwd_tma, P.n_items)), dim3(NT), args,
+                                  k.smem_fwd_tma, st_));
+        return 0;
+    }
     void *args[] = {(void *)&p};
     OTF_CUDA(cudaLaunchKernel((const void *)(with_ring ? k.fwd_ring : k.fwd), grid, dim3(NT),
                               args, k.smem, st_));
     return 0;
 }
 
-int Engine::launch_reverse_step(const StepParams &p, dim3 grid)
+// One reverse step launch: set 0 reads P from slot pin, A from ain; set 1 reads slot in1.
+int Engine::launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain, int in1)
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
+    if (use_tma(k, variant_)) {
+        TmaParams P = *tmap_;
+        P.p = p;
+        P.s0_p_in = pin;
+        P.s0_a_in = ain;
+        P.s1_in = in1;
+        P.n_tiles = (int)grid.x;
+        P.n_items = (int)(grid.x * grid.y);
+        P.err = derr_;
+        void *args[] = {(void *)&P};
+        OTF_CUDA(cudaLaunchKernel((const void *)k.rev_tma, dim3(std::min(k.grid_rev_tma, P.n_items)),
+                                  dim3(NT), args, k.smem_rev_tma, st_));
+        return 0;
+    }
     void *args[] = {(void *)&p};
     OTF_CUDA(cudaLaunchKernel((const void *)k.rev, grid, dim3(NT), args, k.smem, st_));
+    return 0;
+}
+
+// Tensor maps of every field buffer and slot (boxes of the current tile shape).
+int Engine::build_maps()
+{
+    if (!tmap_) {
+        tmap_ = new (std::nothrow) TmaParams();
+        OTF_CHECK(tmap_ != nullptr, 2, "host allocation of the tensor-map block failed");
+    }
+    memset((void *)tmap_, 0, sizeof(TmaParams));
+    const TileShape ts = kTileShapes[cfg_.tile];
+    const int TX = ts.tx, TZ = ts.tz, S = cfg_.max_shots;
+    SetMaps *sets[2] = {&tmap_->s0, &tmap_->s1};
+    for (int s = 0; s < 2; s++)
+        for (int l = 0; l < 2; l++) {
+            if (encode_map(&sets[s]->px[l], fld_[s][0][l], L_, S, TX + 8, TZ + 8) ||
+                encode_map(&sets[s]->pz[l], fld_[s][1][l], L_, S, TX + 8, TZ + 8) ||
+                encode_map(&sets[s]->ax[l], fld_[s][2][l], L_, S, TX + 16, TZ + 8) ||
+                encode_map(&sets[s]->az[l], fld_[s][3][l], L_, S, TX + 8, TZ + 16))
+                return -1;
+        }
+    if (encode_map(&tmap_->qf, qf_, L_, 1, TX + 8, TZ + 8) ||
+        encode_map(&tmap_->qr, qr_, L_, 1, TX + 8, TZ + 8) ||
+        encode_map(&tmap_->grad, grad_, L_, S, TX, TZ))
+        return -1;
+    maps_dirty_ = false;
+    return 0;
+}
+
+int Engine::set_variant(int variant)
+{
+    OTF_CHECK(variant == 0 || variant == 1, 1, "unknown kernel variant");
+    if (variant != variant_) {
+        variant_ = variant;
+        drop_graphs();
+    }
     return 0;
 }
 
@@ -679,7 +825,7 @@ int Engine::emit_forward(bool with_ring)
         p.t = t;
         p.f0 = Fields{fld_[0][0][i], fld_[0][1][i], fld_[0][2][i], fld_[0][3][i],
                       fld_[0][0][o], fld_[0][1][o], fld_[0][2][o], fld_[0][3][o]};
-        if (launch_forward_step(p, with_ring, grid))
+        if (launch_forward_step(p, with_ring, grid, i, i))
             return -1;
     }
     return 0;
@@ -720,7 +866,7 @@ int Engine::emit_reverse()
                       fld_[0][0][po], fld_[0][1][po], fld_[0][2][ao], fld_[0][3][ao]};
         p.f1 = Fields{fld_[1][0][i], fld_[1][1][i], fld_[1][2][i], fld_[1][3][i],
                       fld_[1][0][o], fld_[1][1][o], fld_[1][2][o], fld_[1][3][o]};
-        if (launch_reverse_step(p, grid))
+        if (launch_reverse_step(p, grid, pi, ai, i))
             return -1;
     }
     return 0;
@@ -751,6 +897,8 @@ int Engine::prepare()
     OTF_CHECK(ready_, 2, "engine not initialised");
     OTF_CHECK(!shot_ptr_.empty(), 2, "no shots configured");
     if (tables_dirty_ && build_tables())
+        return -1;
+    if (variant_in_use() == 1 && maps_dirty_ && build_maps())
         return -1;
     return 0;
 }
@@ -835,6 +983,14 @@ int Engine::grad_sum(float *dst, float scale)
 int Engine::sync()
 {
     OTF_CUDA(cudaStreamSynchronize(st_));
+    if (derr_) {
+        int h = 0;
+        OTF_CUDA(cudaMemcpy(&h, derr_, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) {
+            OTF_CUDA(cudaMemset(derr_, 0, sizeof(int)));
+            OTF_CHECK(false, 5, "a bounded wait for tensor-memory copies timed out in a step kernel");
+        }
+    }
     return 0;
 }
 

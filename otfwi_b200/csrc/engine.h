@@ -6,6 +6,7 @@
 #include <vector>
 #include "otf_common.cuh"
 #include "pml_step.cuh"
+#include "pml_step_tma.cuh"
 
 namespace otf {
 
@@ -15,7 +16,7 @@ enum Precision : int { kFaithful = 0, kFast = 1 };
 struct TileShape {
     int tx, tz;
 };
-constexpr int kNumTileShapes = 4;
+constexpr int kNumTileShapes = 5;
 extern const TileShape kTileShapes[kNumTileShapes];
 
 struct EngineConfig {
@@ -77,17 +78,23 @@ class Engine {
     const Layout &layout() const { return L_; }
     int set_precision(int prec);
     int set_tile(int tile);
+    // 0: one tile per CTA; 1: persistent TMA-pipelined kernels where the tile
+    // shape supports them (default)
+    int set_variant(int variant);
+    int variant_in_use() const;
+    // waits for the stream and reports a timed-out bounded wait in a kernel
     int sync();
 
   private:
     int build_tables();
+    int build_maps();
     int prepare();
     int emit_forward(bool with_ring);
     int emit_reverse();
     template <class Emit>
     int capture(cudaGraphExec_t *out, Emit emit);
-    int launch_forward_step(const StepParams &p, bool with_ring, dim3 grid);
-    int launch_reverse_step(const StepParams &p, dim3 grid);
+    int launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, int pin, int ain);
+    int launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain, int in1);
     void drop_graphs();
     StepParams base_params() const;
     void free_all();
@@ -132,6 +139,11 @@ class Engine {
     double *tot_ = nullptr;  // misfit total of the last gradient()
     int graph_shots_ = -1;
     bool tables_dirty_ = true;
+
+    int variant_ = 1;
+    int *derr_ = nullptr;         // device error flag of the bounded waits
+    TmaParams *tmap_ = nullptr;   // tensor maps of every field, slot and coefficient
+    bool maps_dirty_ = true;
 };
 
 }  // namespace otf

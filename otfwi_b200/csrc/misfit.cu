@@ -185,10 +185,10 @@ __device__ __forceinline__ double tval(int i, int T, double step)
     return i == T - 1 ? 1.0 : (double)i * step;  // numpy linspace(0, 1, T)
 }
 
-__device__ __forceinline__ double softplus_d(double x, double s)
+// log(1 + exp(y)) without overflow
+__device__ __forceinline__ double softplus_unit(double y)
 {
-    const double y = x / s;
-    return s * (fmax(y, 0.0) + log1p(exp(-fabs(y))));
+    return fmax(y, 0.0) + log1p(exp(-fabs(y)));
 }
 
 // Stable ascending sort of (key, index) pairs of length n (padded to a power
@@ -251,24 +251,35 @@ __global__ void __launch_bounds__(MT) k_wasserstein(const float *__restrict__ si
     const double step = 1.0 / (double)(T - 1);
     // per-trace transform parameters, from the observed trace only
     double c = 0.0, s = 1.0;
+    float scale = 1.f;
     {
-        float mn = __int_as_float(0x7f800000), mx = -mn, am = 0.f;
+        float mn = __int_as_float(0x7f800000), mx = -mn, am = 0.f, af = 0.f;
         for (int i = threadIdx.x; i < T; i += MT) {
             mn = fminf(mn, g[i]);
             mx = fmaxf(mx, g[i]);
             am = fmaxf(am, fabsf(g[i]));
+            af = fmaxf(af, fabsf(f[i]));
         }
         mn = block_minmax(mn, false, redf);
         mx = block_minmax(mx, true, redf);
         am = block_minmax(am, true, redf);
+        af = block_minmax(af, true, redf);
         c = fmax(-1.1 * (double)mn, 0.1 * (double)mx);  // adjoint_functions.py:38-39
         s = am > 0.f ? 0.1 * (double)am : 1.0;
+        // The normalisation p = f / sum(f dt) is scale-free, so the shifted
+        // traces are brought to unit magnitude by an exact power of two:
+        // float-float keeps FP64-class precision only for normal magnitudes.
+        const double m = fmax(fmax((double)am, (double)af), fabs(c));
+        if (m > 0.0 && m < 1e30)
+            scale = ldexpf(1.f, -ilogb(m));
     }
+    // densities up to a constant factor (scale for kind 1, 1/s for kind 2)
+    const double cs = c * (double)scale;
     auto pf = [&](int i) -> FF {
-        return KIND == 1 ? add(ff(f[i]), ffd(c)) : ffd(softplus_d((double)f[i], s));
+        return KIND == 1 ? add(ff(__fmul_rn(f[i], scale)), ffd(cs)) : ffd(softplus_unit((double)f[i] / s));
     };
     auto pg = [&](int i) -> FF {
-        return KIND == 1 ? add(ff(g[i]), ffd(c)) : ffd(softplus_d((double)g[i], s));
+        return KIND == 1 ? add(ff(__fmul_rn(g[i], scale)), ffd(cs)) : ffd(softplus_unit((double)g[i] / s));
     };
     // normalisation: divide by sum(p * dt) (adjoint_functions.py:43-44)
     FF sf{0.f, 0.f}, sg{0.f, 0.f};
@@ -341,9 +352,10 @@ __global__ void __launch_bounds__(MT) k_wasserstein(const float *__restrict__ si
         for (int i = threadIdx.x; i < T; i += MT)
             m = add(m, mul(sub(Fs[i], last), div(pf(i), Zf)));
         m = mul(block_sum(m, red), dtf);
+        // Zf holds Z / s (densities were built as softplus(f/s))
         for (int i = threadIdx.x; i < T; i += MT) {
             const double sig = 0.5 * (1.0 + tanh(0.5 * (double)f[i] / s));
-            a[i] = __double2float_rn(sig / ff2d(Zf) * ff2d(sub(sub(Fs[i], last), m)));
+            a[i] = __double2float_rn(sig / (s * ff2d(Zf)) * ff2d(sub(sub(Fs[i], last), m)));
         }
     }
     if (threadIdx.x == 0)

@@ -143,8 +143,12 @@ struct TileGeom {
     static constexpr int EX = TX + 8, EZ = TZ + 8;      // P(t) region (tile + 4-cell halo)
     static constexpr int AXW = TX + 16, AXH = TZ + 8;   // Ax(t-1) tile: x halo 8, z halo 4
     static constexpr int AZW = TX + 8, AZH = TZ + 16;   // Az(t-1) tile: x halo 4, z halo 8
-    static constexpr int SAX = 0, SAZ = AXW * AXH, SPX = SAZ + AZW * AZH, SPZ = SPX + EX * EZ;
-    static constexpr int SMEM_FLOATS = SPZ + EX * EZ;
+    static constexpr int NAX = AXW * AXH, NAZ = AZW * AZH, NE = EX * EZ, NO = TX * TZ;
+    // v1 layout (one tile, A staged by the CTA itself)
+    static constexpr int SAX = 0, SAZ = NAX, SPX = SAZ + NAZ, SPZ = SPX + NE;
+    static constexpr int SMEM_FLOATS = SPZ + NE;
+    // v2 stage (all inputs of one field set staged by TMA): Ax | Az | Px(t-1) | Pz(t-1) | q
+    static constexpr int STAGE_FLOATS = NAX + NAZ + 3 * NE;
     static constexpr int NBEX = EX / 4, NBE = NBEX * (EZ / 4);  // 4x4 blocks of the P region
     static constexpr int NBOX = TX / 4, NBO = NBOX * (TZ / 4);  // 4x4 blocks of the owned tile
     static constexpr int KO = (NBO + NT - 1) / NT;               // owned blocks per thread
@@ -153,6 +157,10 @@ struct TileGeom {
 __device__ __forceinline__ float4 ld4(const float *base, int64_t idx)
 {
     return __ldg(reinterpret_cast<const float4 *>(base + idx));
+}
+__device__ __forceinline__ float4 lds4(const float *base, int idx)
+{
+    return *reinterpret_cast<const float4 *>(base + idx);
 }
 __device__ __forceinline__ void f4a(const float4 v, float *a)
 {
@@ -163,14 +171,14 @@ __device__ __forceinline__ void f4a(const float4 v, float *a)
 }
 
 // Stage A(t-1) tiles (with halo) from global into shared memory, coalesced
-// 16-byte loads; outside the allocation reads as zero.
+// 16-byte loads; outside the allocation reads as zero (v1 kernels).
 template <int TX, int TZ>
-__device__ __forceinline__ void load_a_tiles(const StepParams &p, float *sm, const float *ax,
-                                             const float *az, int x0, int z0)
+__device__ __forceinline__ void load_a_tiles(const StepParams &p, float *sAx_, float *sAz_,
+                                             const float *ax, const float *az, int x0, int z0)
 {
     using G = TileGeom<TX, TZ>;
-    float4 *sAx = reinterpret_cast<float4 *>(sm + G::SAX);
-    float4 *sAz = reinterpret_cast<float4 *>(sm + G::SAZ);
+    float4 *sAx = reinterpret_cast<float4 *>(sAx_);
+    float4 *sAz = reinterpret_cast<float4 *>(sAz_);
     constexpr int AXW4 = G::AXW / 4, AZW4 = G::AZW / 4;
     for (int i = threadIdx.x; i < AXW4 * G::AXH; i += NT) {
         const int rr = i / AXW4, cc = i - rr * AXW4;
@@ -196,33 +204,32 @@ __device__ __forceinline__ bool inb(const StepParams &p, int x, int z)
 }
 
 // P half-step over the halo-extended region (simulateFrameP,
-// regression_PML_single.cu:503-519).
-template <int TX, int TZ, class Prec, bool SEP, bool REVERT>
-__device__ __forceinline__ void p_phase(const StepParams &p, float *sm, const float *px_in,
+// regression_PML_single.cu:503-519), into sPx / sPz.
+// TILED: P(t-1) and q are read from shared-memory E tiles (row stride EX);
+// otherwise from the padded global arrays.
+template <int TX, int TZ, class Prec, bool SEP, bool REVERT, bool TILED>
+__device__ __forceinline__ void p_phase(const StepParams &p, const float *sAx, const float *sAz,
+                                        float *sPx, float *sPz, const float *px_in,
                                         const float *pz_in, const float *q, int x0, int z0)
 {
     using G = TileGeom<TX, TZ>;
-    const float *sAx = sm + G::SAX;
-    const float *sAz = sm + G::SAZ;
-    float *sPx = sm + G::SPX;
-    float *sPz = sm + G::SPZ;
     for (int b = threadIdx.x; b < G::NBE; b += NT) {
         const int ex = 4 * (b % G::NBEX), ez = 4 * (b / G::NBEX);
         float dAx[4][4], dAz[4][4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             float w[12];
-            const float4 *row = reinterpret_cast<const float4 *>(sAx + (ez + i) * G::AXW + ex);
-            f4a(row[0], w);
-            f4a(row[1], w + 4);
-            f4a(row[2], w + 8);
+            const float *row = sAx + (ez + i) * G::AXW + ex;
+            f4a(lds4(row, 0), w);
+            f4a(lds4(row, 4), w + 4);
+            f4a(lds4(row, 8), w + 8);
             Prec::dstag4(w, dAx[i]);
         }
         {
             float wz[4][11];
 #pragma unroll
             for (int k = 0; k < 11; k++) {
-                const float4 v = *reinterpret_cast<const float4 *>(sAz + (ez + k) * G::AZW + ex);
+                const float4 v = lds4(sAz, (ez + k) * G::AZW + ex);
                 wz[0][k] = v.x;
                 wz[1][k] = v.y;
                 wz[2][k] = v.z;
@@ -251,18 +258,24 @@ __device__ __forceinline__ void p_phase(const StepParams &p, float *sm, const fl
             float dx2[4] = {1.f, 1.f, 1.f, 1.f}, dz2[4] = {1.f, 1.f, 1.f, 1.f};
             float dmz = 1.f;
             const bool ok = prow < p.rows && pcol < p.pitch;
-            if (ok) {
+            if (TILED) {
+                const int e = (ez + i) * G::EX + ex;
+                f4a(lds4(px_in, e), po_x);
+                f4a(lds4(pz_in, e), po_z);
+                f4a(lds4(q, e), qv);
+            } else if (ok) {
                 const int64_t o = (int64_t)prow * p.pitch + pcol;
                 f4a(ld4(px_in, o), po_x);
                 f4a(ld4(pz_in, o), po_z);
                 f4a(ld4(q, o), qv);
-                if (!REVERT) {
-                    if (SEP) {
-                        dmz = __ldg(p.dampz + prow);
-                    } else {
-                        f4a(ld4(p.dampx2, o), dx2);
-                        f4a(ld4(p.dampz2, o), dz2);
-                    }
+            }
+            if (!REVERT && ok) {
+                if (SEP) {
+                    dmz = __ldg(p.dampz + prow);
+                } else {
+                    const int64_t o = (int64_t)prow * p.pitch + pcol;
+                    f4a(ld4(p.dampx2, o), dx2);
+                    f4a(ld4(p.dampz2, o), dz2);
                 }
             }
             float nx[4], nz[4];
@@ -291,11 +304,10 @@ __device__ __forceinline__ void p_phase(const StepParams &p, float *sm, const fl
 // Point injection into P(t) in shared memory (somaFonteIntegral,
 // regression_PML_single.cu:285-291): P += I(t)/2 on both split components.
 template <int TX, int TZ>
-__device__ __forceinline__ void inject(const StepParams &p, float *sm, int shot, int x0, int z0)
+__device__ __forceinline__ void inject(const StepParams &p, float *sPx, float *sPz, int shot, int x0,
+                                       int z0)
 {
     using G = TileGeom<TX, TZ>;
-    float *sPx = sm + G::SPX;
-    float *sPz = sm + G::SPZ;
     const int b = p.inj_ptr[shot], e = p.inj_ptr[shot + 1];
     for (int k = b + threadIdx.x; k < e; k += NT) {
         const int ex = p.inj_x[k] - (x0 - 4), ez = p.inj_z[k] - (z0 - 4);
@@ -307,14 +319,49 @@ __device__ __forceinline__ void inject(const StepParams &p, float *sm, int shot,
     }
 }
 
-// Write P(t) of the owned tile from shared memory to the output slot.
+// setRec (regression_PML_single.cu:269-270): ring cells of the E region <- ring(T-1-t)/2
 template <int TX, int TZ>
-__device__ __forceinline__ void store_p(const StepParams &p, const float *sm, float *px_out,
-                                        float *pz_out, int x0, int z0)
+__device__ __forceinline__ void ring_overwrite(const StepParams &p, float *sPx, float *sPz, int shot,
+                                               int tile)
+{
+    const float *ring = p.ring + ((int64_t)shot * p.T + (p.T - 1 - p.t)) * p.n_ring;
+    for (int e = p.ringe_ptr[tile] + threadIdx.x; e < p.ringe_ptr[tile + 1]; e += NT) {
+        const float v = __fmul_rn(ring[p.ringe_id[e]], 0.5f);
+        sPx[p.ringe_cell[e]] = v;
+        sPz[p.ringe_cell[e]] = v;
+    }
+}
+
+// Receivers (and with RING the boundary ring) at owned cells, after injection
+// (gravaBufferSensores, regression_PML_single.cu:758-759).
+template <int TX, int TZ, bool RING>
+__device__ __forceinline__ void record(const StepParams &p, const float *sPx, const float *sPz,
+                                       int shot, int tile)
 {
     using G = TileGeom<TX, TZ>;
-    const float *sPx = sm + G::SPX;
-    const float *sPz = sm + G::SPZ;
+    for (int e = p.sen_ptr[tile] + threadIdx.x; e < p.sen_ptr[tile + 1]; e += NT) {
+        const int c = p.sen_cell[e];
+        const int oz = c / TX, ox = c - oz * TX;
+        const int s = (oz + 4) * G::EX + ox + 4;
+        p.rec[((int64_t)shot * p.n_sen + p.sen_id[e]) * p.T + p.t] = __fadd_rn(sPx[s], sPz[s]);
+    }
+    if (RING) {
+        float *ring = p.ring + ((int64_t)shot * p.T + p.t) * p.n_ring;
+        for (int e = p.ringo_ptr[tile] + threadIdx.x; e < p.ringo_ptr[tile + 1]; e += NT) {
+            const int c = p.ringo_cell[e];
+            const int oz = c / TX, ox = c - oz * TX;
+            const int s = (oz + 4) * G::EX + ox + 4;
+            ring[e] = __fadd_rn(sPx[s], sPz[s]);
+        }
+    }
+}
+
+// Write P(t) of the owned tile from shared memory to the output slot.
+template <int TX, int TZ>
+__device__ __forceinline__ void store_p(const StepParams &p, const float *sPx, const float *sPz,
+                                        float *px_out, float *pz_out, int x0, int z0)
+{
+    using G = TileGeom<TX, TZ>;
     constexpr int W4 = TX / 4;
     for (int i = threadIdx.x; i < W4 * TZ; i += NT) {
         const int oz = i / W4, ox = 4 * (i - oz * W4);
@@ -322,24 +369,24 @@ __device__ __forceinline__ void store_p(const StepParams &p, const float *sm, fl
         if (prow < p.rows && pcol < p.pitch) {
             const int64_t o = (int64_t)prow * p.pitch + pcol;
             const int s = (oz + 4) * G::EX + ox + 4;
-            *reinterpret_cast<float4 *>(px_out + o) = *reinterpret_cast<const float4 *>(sPx + s);
-            *reinterpret_cast<float4 *>(pz_out + o) = *reinterpret_cast<const float4 *>(sPz + s);
+            *reinterpret_cast<float4 *>(px_out + o) = lds4(sPx, s);
+            *reinterpret_cast<float4 *>(pz_out + o) = lds4(sPz, s);
         }
     }
 }
 
 // A half-step at owned cells (simulateFrameA, regression_PML_single.cu:587-608).
-// With LAP, also returns lap9(Px + Pz) at the owned cells (calcGrad2's
-// operand, regression_PML_single.cu:442) in lap[k] for the k-th owned block
-// this thread handles.
-template <int TX, int TZ, class Prec, bool SEP, bool REVERT, bool LAP>
-__device__ __forceinline__ void a_phase(const StepParams &p, const float *sm, const float *ax_in,
+// TILED: A(t-1) at owned cells is read from the staged A tiles; otherwise
+// from global. With LAP, also returns lap9(Px + Pz) at the owned cells
+// (calcGrad2's operand, regression_PML_single.cu:442) in lap[k] for the k-th
+// owned block this thread handles.
+template <int TX, int TZ, class Prec, bool SEP, bool REVERT, bool LAP, bool TILED>
+__device__ __forceinline__ void a_phase(const StepParams &p, const float *sAx, const float *sAz,
+                                        const float *sPx, const float *sPz, const float *ax_in,
                                         const float *az_in, float *ax_out, float *az_out, int x0,
                                         int z0, float (*lap)[16])
 {
     using G = TileGeom<TX, TZ>;
-    const float *sPx = sm + G::SPX;
-    const float *sPz = sm + G::SPZ;
 #pragma unroll
     for (int k = 0; k < G::KO; k++) {
         const int b = threadIdx.x + k * NT;
@@ -351,14 +398,13 @@ __device__ __forceinline__ void a_phase(const StepParams &p, const float *sm, co
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             float wx[12], wz[12], ox4[4], oz4[4];
-            const float4 *rx = reinterpret_cast<const float4 *>(sPx + (oz + 4 + i) * G::EX + ox);
-            const float4 *rz = reinterpret_cast<const float4 *>(sPz + (oz + 4 + i) * G::EX + ox);
-            f4a(rx[0], wx);
-            f4a(rx[1], wx + 4);
-            f4a(rx[2], wx + 8);
-            f4a(rz[0], wz);
-            f4a(rz[1], wz + 4);
-            f4a(rz[2], wz + 8);
+            const int r = (oz + 4 + i) * G::EX + ox;
+            f4a(lds4(sPx, r), wx);
+            f4a(lds4(sPx, r + 4), wx + 4);
+            f4a(lds4(sPx, r + 8), wx + 8);
+            f4a(lds4(sPz, r), wz);
+            f4a(lds4(sPz, r + 4), wz + 4);
+            f4a(lds4(sPz, r + 8), wz + 8);
             Prec::dstag4(wx + 1, ox4);
             Prec::dstag4(wz + 1, oz4);
 #pragma unroll
@@ -380,8 +426,8 @@ __device__ __forceinline__ void a_phase(const StepParams &p, const float *sm, co
             float vx[4][11], vz[4][11];
 #pragma unroll
             for (int c = 0; c < 11; c++) {
-                const float4 a = *reinterpret_cast<const float4 *>(sPx + (oz + 1 + c) * G::EX + ox + 4);
-                const float4 bq = *reinterpret_cast<const float4 *>(sPz + (oz + 1 + c) * G::EX + ox + 4);
+                const float4 a = lds4(sPx, (oz + 1 + c) * G::EX + ox + 4);
+                const float4 bq = lds4(sPz, (oz + 1 + c) * G::EX + ox + 4);
                 vx[0][c] = a.x; vx[1][c] = a.y; vx[2][c] = a.z; vx[3][c] = a.w;
                 vz[0][c] = bq.x; vz[1][c] = bq.y; vz[2][c] = bq.z; vz[3][c] = bq.w;
             }
@@ -400,8 +446,8 @@ __device__ __forceinline__ void a_phase(const StepParams &p, const float *sm, co
             float vs[4][12];
 #pragma unroll
             for (int c = 0; c < 12; c++) {
-                const float4 a = *reinterpret_cast<const float4 *>(sPx + (oz + c) * G::EX + ox + 4);
-                const float4 bq = *reinterpret_cast<const float4 *>(sPz + (oz + c) * G::EX + ox + 4);
+                const float4 a = lds4(sPx, (oz + c) * G::EX + ox + 4);
+                const float4 bq = lds4(sPz, (oz + c) * G::EX + ox + 4);
                 vs[0][c] = __fadd_rn(a.x, bq.x);
                 vs[1][c] = __fadd_rn(a.y, bq.y);
                 vs[2][c] = __fadd_rn(a.z, bq.z);
@@ -427,8 +473,13 @@ __device__ __forceinline__ void a_phase(const StepParams &p, const float *sm, co
                 continue;
             const int64_t o = (int64_t)prow * p.pitch + pcol;
             float ao_x[4], ao_z[4];
-            f4a(ld4(ax_in, o), ao_x);
-            f4a(ld4(az_in, o), ao_z);
+            if (TILED) {
+                f4a(lds4(sAx, (oz + 4 + i) * G::AXW + ox + 8), ao_x);
+                f4a(lds4(sAz, (oz + 8 + i) * G::AZW + ox + 4), ao_z);
+            } else {
+                f4a(ld4(ax_in, o), ao_x);
+                f4a(ld4(az_in, o), ao_z);
+            }
             float dx2[4] = {1.f, 1.f, 1.f, 1.f}, dz2[4] = {1.f, 1.f, 1.f, 1.f};
             float dmz = 1.f;
             if (!REVERT) {
@@ -462,11 +513,43 @@ __device__ __forceinline__ void a_phase(const StepParams &p, const float *sm, co
     }
 }
 
-template <class T>
-__device__ __forceinline__ T *shot_ptr(T *base, int64_t stride, int shot)
+// Imaging condition at owned cells (calcGrad2, regression_PML_single.cu:442-443):
+// grad += (Px + Pz)(t) * lap. g_in: shared tile (row stride TX) when TILED,
+// else the global gradient itself.
+template <int TX, int TZ, bool TILED>
+__device__ __forceinline__ void image(const StepParams &p, const float *sPx, const float *sPz,
+                                      const float *g_tile, float *grad, int x0, int z0,
+                                      const float (*lap)[16])
 {
-    return base + stride * shot;
+    using G = TileGeom<TX, TZ>;
+#pragma unroll
+    for (int k = 0; k < G::KO; k++) {
+        const int b = threadIdx.x + k * NT;
+        if (b >= G::NBO)
+            break;
+        const int ox = 4 * (b % G::NBOX), oz = 4 * (b / G::NBOX);
+        const int pcol = x0 + ox + PAD;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int prow = z0 + oz + i + PAD;
+            if (prow >= p.rows || pcol >= p.pitch)
+                continue;
+            const int64_t o = (int64_t)prow * p.pitch + pcol;
+            const float4 a = lds4(sPx, (oz + 4 + i) * G::EX + ox + 4);
+            const float4 bq = lds4(sPz, (oz + 4 + i) * G::EX + ox + 4);
+            float4 g = TILED ? lds4(g_tile, (oz + i) * TX + ox) : *reinterpret_cast<float4 *>(grad + o);
+            g.x = __fmaf_rn(__fadd_rn(a.x, bq.x), lap[k][i * 4 + 0], g.x);
+            g.y = __fmaf_rn(__fadd_rn(a.y, bq.y), lap[k][i * 4 + 1], g.y);
+            g.z = __fmaf_rn(__fadd_rn(a.z, bq.z), lap[k][i * 4 + 2], g.z);
+            g.w = __fmaf_rn(__fadd_rn(a.w, bq.w), lap[k][i * 4 + 3], g.w);
+            *reinterpret_cast<float4 *>(grad + o) = g;
+        }
+    }
 }
+
+// ---------------------------------------------------------------------------
+// v1 kernels: one launch per time step, one tile per CTA, A(t-1) staged by
+// the CTA's own loads.
 
 // Forward step: cuda_simulate / cuda_grad_ext phase 1 body
 // (regression_PML_single.cu:661-677, 745-764): P update, source injection,
@@ -477,39 +560,23 @@ __global__ void __launch_bounds__(NT) k_forward_step(const StepParams p)
     extern __shared__ float4 smem4[];
     float *sm = reinterpret_cast<float *>(smem4);
     using G = TileGeom<TX, TZ>;
+    float *sAx = sm + G::SAX, *sAz = sm + G::SAZ, *sPx = sm + G::SPX, *sPz = sm + G::SPZ;
     const int tile = blockIdx.x, shot = blockIdx.y;
     const int x0 = (tile % p.ntx) * TX, z0 = (tile / p.ntx) * TZ;
     const int64_t so = p.shot_stride * shot;
     const Fields &f = p.f0;
 
-    load_a_tiles<TX, TZ>(p, sm, f.ax_in + so, f.az_in + so, x0, z0);
+    load_a_tiles<TX, TZ>(p, sAx, sAz, f.ax_in + so, f.az_in + so, x0, z0);
     __syncthreads();
-    p_phase<TX, TZ, Prec, SEP, false>(p, sm, f.px_in + so, f.pz_in + so, p.q0, x0, z0);
+    p_phase<TX, TZ, Prec, SEP, false, false>(p, sAx, sAz, sPx, sPz, f.px_in + so, f.pz_in + so, p.q0,
+                                             x0, z0);
     __syncthreads();
-    inject<TX, TZ>(p, sm, shot, x0, z0);
+    inject<TX, TZ>(p, sPx, sPz, shot, x0, z0);
     __syncthreads();
-    store_p<TX, TZ>(p, sm, f.px_out + so, f.pz_out + so, x0, z0);
-    {
-        const float *sPx = sm + G::SPX;
-        const float *sPz = sm + G::SPZ;
-        for (int e = p.sen_ptr[tile] + threadIdx.x; e < p.sen_ptr[tile + 1]; e += NT) {
-            const int c = p.sen_cell[e];
-            const int oz = c / TX, ox = c - oz * TX;
-            const int s = (oz + 4) * G::EX + ox + 4;
-            p.rec[((int64_t)shot * p.n_sen + p.sen_id[e]) * p.T + p.t] = __fadd_rn(sPx[s], sPz[s]);
-        }
-        if (RING) {
-            float *ring = p.ring + ((int64_t)shot * p.T + p.t) * p.n_ring;
-            for (int e = p.ringo_ptr[tile] + threadIdx.x; e < p.ringo_ptr[tile + 1]; e += NT) {
-                const int c = p.ringo_cell[e];
-                const int oz = c / TX, ox = c - oz * TX;
-                const int s = (oz + 4) * G::EX + ox + 4;
-                ring[e] = __fadd_rn(sPx[s], sPz[s]);
-            }
-        }
-    }
-    a_phase<TX, TZ, Prec, SEP, false, false>(p, sm, f.ax_in + so, f.az_in + so, f.ax_out + so,
-                                             f.az_out + so, x0, z0, nullptr);
+    store_p<TX, TZ>(p, sPx, sPz, f.px_out + so, f.pz_out + so, x0, z0);
+    record<TX, TZ, RING>(p, sPx, sPz, shot, tile);
+    a_phase<TX, TZ, Prec, SEP, false, false, false>(p, sAx, sAz, sPx, sPz, f.ax_in + so, f.az_in + so,
+                                                    f.ax_out + so, f.az_out + so, x0, z0, nullptr);
 }
 
 // Reverse step: cuda_grad_ext phase 2 body (regression_PML_single.cu:795-825)
@@ -523,73 +590,39 @@ __global__ void __launch_bounds__(NT) k_reverse_step(const StepParams p)
     extern __shared__ float4 smem4[];
     float *sm = reinterpret_cast<float *>(smem4);
     using G = TileGeom<TX, TZ>;
+    float *sAx = sm + G::SAX, *sAz = sm + G::SAZ, *sPx = sm + G::SPX, *sPz = sm + G::SPZ;
     const int tile = blockIdx.x, shot = blockIdx.y;
     const int x0 = (tile % p.ntx) * TX, z0 = (tile / p.ntx) * TZ;
     const int64_t so = p.shot_stride * shot;
     float lap[G::KO][16];
 
     // reconstruction
-    load_a_tiles<TX, TZ>(p, sm, p.f0.ax_in + so, p.f0.az_in + so, x0, z0);
+    load_a_tiles<TX, TZ>(p, sAx, sAz, p.f0.ax_in + so, p.f0.az_in + so, x0, z0);
     __syncthreads();
-    p_phase<TX, TZ, Prec, SEP, true>(p, sm, p.f0.px_in + so, p.f0.pz_in + so, p.q0, x0, z0);
+    p_phase<TX, TZ, Prec, SEP, true, false>(p, sAx, sAz, sPx, sPz, p.f0.px_in + so, p.f0.pz_in + so,
+                                            p.q0, x0, z0);
     __syncthreads();
-    {
-        // setRec (regression_PML_single.cu:269-270): ring cells <- ring(T-1-t)/2
-        float *sPx = sm + G::SPX;
-        float *sPz = sm + G::SPZ;
-        const float *ring = p.ring + ((int64_t)shot * p.T + (p.T - 1 - p.t)) * p.n_ring;
-        for (int e = p.ringe_ptr[tile] + threadIdx.x; e < p.ringe_ptr[tile + 1]; e += NT) {
-            const float v = __fmul_rn(ring[p.ringe_id[e]], 0.5f);
-            sPx[p.ringe_cell[e]] = v;
-            sPz[p.ringe_cell[e]] = v;
-        }
-    }
+    ring_overwrite<TX, TZ>(p, sPx, sPz, shot, tile);
     __syncthreads();
-    store_p<TX, TZ>(p, sm, p.f0.px_out + so, p.f0.pz_out + so, x0, z0);
-    a_phase<TX, TZ, Prec, SEP, true, true>(p, sm, p.f0.ax_in + so, p.f0.az_in + so,
-                                           p.f0.ax_out + so, p.f0.az_out + so, x0, z0, lap);
+    store_p<TX, TZ>(p, sPx, sPz, p.f0.px_out + so, p.f0.pz_out + so, x0, z0);
+    a_phase<TX, TZ, Prec, SEP, true, true, false>(p, sAx, sAz, sPx, sPz, p.f0.ax_in + so,
+                                                  p.f0.az_in + so, p.f0.ax_out + so, p.f0.az_out + so,
+                                                  x0, z0, lap);
     __syncthreads();
 
     // adjoint
-    load_a_tiles<TX, TZ>(p, sm, p.f1.ax_in + so, p.f1.az_in + so, x0, z0);
+    load_a_tiles<TX, TZ>(p, sAx, sAz, p.f1.ax_in + so, p.f1.az_in + so, x0, z0);
     __syncthreads();
-    p_phase<TX, TZ, Prec, SEP, false>(p, sm, p.f1.px_in + so, p.f1.pz_in + so, p.q1, x0, z0);
+    p_phase<TX, TZ, Prec, SEP, false, false>(p, sAx, sAz, sPx, sPz, p.f1.px_in + so, p.f1.pz_in + so,
+                                             p.q1, x0, z0);
     __syncthreads();
-    inject<TX, TZ>(p, sm, shot, x0, z0);
+    inject<TX, TZ>(p, sPx, sPz, shot, x0, z0);
     __syncthreads();
-    store_p<TX, TZ>(p, sm, p.f1.px_out + so, p.f1.pz_out + so, x0, z0);
-    a_phase<TX, TZ, Prec, SEP, false, false>(p, sm, p.f1.ax_in + so, p.f1.az_in + so,
-                                             p.f1.ax_out + so, p.f1.az_out + so, x0, z0, nullptr);
-
-    // imaging condition (calcGrad2, regression_PML_single.cu:442-443)
-    {
-        const float *sPx = sm + G::SPX;
-        const float *sPz = sm + G::SPZ;
-        float *grad = p.grad + so;
-#pragma unroll
-        for (int k = 0; k < G::KO; k++) {
-            const int b = threadIdx.x + k * NT;
-            if (b >= G::NBO)
-                break;
-            const int ox = 4 * (b % G::NBOX), oz = 4 * (b / G::NBOX);
-            const int pcol = x0 + ox + PAD;
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const int prow = z0 + oz + i + PAD;
-                if (prow >= p.rows || pcol >= p.pitch)
-                    continue;
-                const int64_t o = (int64_t)prow * p.pitch + pcol;
-                const float4 a = *reinterpret_cast<const float4 *>(sPx + (oz + 4 + i) * G::EX + ox + 4);
-                const float4 bq = *reinterpret_cast<const float4 *>(sPz + (oz + 4 + i) * G::EX + ox + 4);
-                float4 g = *reinterpret_cast<float4 *>(grad + o);
-                g.x = __fmaf_rn(__fadd_rn(a.x, bq.x), lap[k][i * 4 + 0], g.x);
-                g.y = __fmaf_rn(__fadd_rn(a.y, bq.y), lap[k][i * 4 + 1], g.y);
-                g.z = __fmaf_rn(__fadd_rn(a.z, bq.z), lap[k][i * 4 + 2], g.z);
-                g.w = __fmaf_rn(__fadd_rn(a.w, bq.w), lap[k][i * 4 + 3], g.w);
-                *reinterpret_cast<float4 *>(grad + o) = g;
-            }
-        }
-    }
+    store_p<TX, TZ>(p, sPx, sPz, p.f1.px_out + so, p.f1.pz_out + so, x0, z0);
+    a_phase<TX, TZ, Prec, SEP, false, false, false>(p, sAx, sAz, sPx, sPz, p.f1.ax_in + so,
+                                                    p.f1.az_in + so, p.f1.ax_out + so,
+                                                    p.f1.az_out + so, x0, z0, nullptr);
+    image<TX, TZ, false>(p, sPx, sPz, nullptr, p.grad + so, x0, z0, lap);
 }
 
 }  // namespace otf

@@ -81,6 +81,29 @@ def test_batched_wasserstein_matches_host_callback(lib):
     assert abs(mis / sc.n_src - cp.mse[0]) <= 1e-5 * abs(cp.mse[0])
 
 
+@pytest.mark.parametrize("tile", [0, 1, 4])
+def test_batched_kernel_variants_identical_many_shots(lib, tile):
+    """Persistent TMA kernels vs one-tile-per-CTA kernels on a batch whose
+    item count is not a multiple of the persistent grid, fast precision."""
+    from otfwi_b200 import scenarios
+    from otfwi_b200.batch import ShotBatch
+    sc = scenarios.fmc(X=200, Z=168, T=160, n_elem=24, pitch=5, x_first=40)
+    out = []
+    for kernel in (0, 1):
+        b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, prec_deriv=4,
+                      precision=1, tile=tile, kernel=kernel)
+        b.set_model(sc.c_true)
+        obs = b.forward()
+        b.set_observed(obs)
+        b.set_model(sc.c_start)
+        g, m = b.gradient("wasserstein_softplus")
+        out.append((obs, g, m))
+        b.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
+
+
 def test_batched_reverse_with_external_adjoint(lib):
     from otfwi_b200.batch import ShotBatch
     sc = _scenario(n_src=2, T=200)

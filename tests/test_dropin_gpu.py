@@ -31,15 +31,17 @@ def _cases():
     return make_sim_golden.cases()
 
 
-def _run(lib, inp, precision=0, tile=0):
+def _run(lib, inp, precision=0, tile=0, kernel=1):
     from otfwi_b200 import _lib
     os.environ["OTFWI_PRECISION"] = str(precision)
     os.environ["OTFWI_TILE"] = str(tile)
+    os.environ["OTFWI_KERNEL"] = str(kernel)
     try:
         return run_abi(lib, **inp, check=lambda: _lib.check(lib))
     finally:
         os.environ.pop("OTFWI_PRECISION", None)
         os.environ.pop("OTFWI_TILE", None)
+        os.environ.pop("OTFWI_KERNEL", None)
 
 
 def _keys(ref):
@@ -90,25 +92,38 @@ def test_dropin_matches_oracles(lib, name):
     _assert_close(res, oracle_case(inp, "f64"), 1e-5, 1e-4, "faithful vs oracle f64")
 
 
-@pytest.mark.parametrize("tile", [1, 2, 3])
+@pytest.mark.parametrize("tile", [1, 2, 3, 4])
 def test_tile_shapes_bit_identical(lib, tile):
     inp = _cases()["medium"]
-    base = _run(lib, inp, tile=0)
+    base = _run(lib, inp, tile=0, kernel=0)
     res = _run(lib, inp, tile=tile)
     for k in base:
         assert np.array_equal(base[k], res[k]), (tile, k)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("tile", [0, 1, 4])
+def test_persistent_tma_kernels_bit_identical_to_per_tile(lib, tile, precision):
+    """The persistent TMA-pipelined step kernels compute with the same device
+    code as the one-tile-per-CTA kernels: identical results."""
+    inp = _cases()["medium"]
+    a = _run(lib, inp, precision=precision, tile=tile, kernel=0)
+    b = _run(lib, inp, precision=precision, tile=tile, kernel=1)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), (tile, precision, k)
+
+
 def test_odd_grid_sizes_every_tile(lib):
-    """Grids that are not multiples of any tile shape."""
+    """Grids that are not multiples of any tile shape, both kernel variants."""
     import make_sim_golden
     from otfwi_b200 import scenarios
     from otfwi_b200.cuda_interface_pml import pml_damping
     sc = scenarios.small(X=101, Z=77, T=200, n_src=1, n_rec=5, seed=3)
     inp = make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))
     ref = oracle_case(inp, "f32")
-    for tile in range(4):
-        _assert_identical(_run(lib, inp, tile=tile), ref, f"odd grid tile {tile}")
+    for tile in range(5):
+        for kernel in (0, 1):
+            _assert_identical(_run(lib, inp, tile=tile, kernel=kernel), ref, f"odd grid tile {tile} k{kernel}")
 
 
 def test_edge_receiver_records_zero(lib):
