@@ -55,10 +55,12 @@ def parse():
     return ap.parse_args()
 
 
-def workload(args):
+def workload(args, rank=0):
+    """The FMC acquisition of one rank: rank r's array sits 2r cells to the
+    right (each rank inverts its own acquisition of the same specimen)."""
     from otfwi_b200 import scenarios
     return scenarios.fmc(X=args.X, Z=args.X, T=args.T, n_elem=args.shots,
-                         x_first=max(24, args.X // 2 - 3 * args.shots + 3))
+                         x_first=max(24, args.X // 2 - 3 * args.shots + 3) + 2 * rank)
 
 
 def config_block(args, sc, parallelism):
@@ -175,7 +177,8 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     from otfwi_b200.batch import ShotBatch
-    sc = workload(args)
+    from otfwi_b200.distributed import allreduce_sum_
+    sc = workload(args, rank)
     b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, prec_deriv=4,
                   precision=args.precision, tile=args.tile)
     dev = torch.device("cuda", local)
@@ -193,9 +196,10 @@ def run_ours(args):
     def step():
         b.gradient(args.misfit, grad=grad, misfit_out=mis)
         if world > 1:
+            # the FWI gradient is the sum over every rank's acquisition: one
+            # NCCL all-reduce of the X*Z gradient and the misfit per step
             with torch.cuda.stream(stream):
-                dist.all_reduce(grad)
-                dist.all_reduce(mis)
+                allreduce_sum_([grad, mis])
 
     for _ in range(args.warmup):
         step()

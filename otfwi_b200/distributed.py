@@ -1,0 +1,43 @@
+"""Multi-GPU FWI gradient: shots (or whole acquisitions) sharded over ranks,
+one reduction per gradient.
+
+The reference runs every shot serially on one GPU (cuda_interface_pml.py:
+225-236: grad_acc += grad per shot, then / n_source). Shots are
+independent, so each rank computes the gradient sum and misfit sum of its own
+shots and one all-reduce (NCCL over NVLink between GPUs; gloo on CPU in the
+tests) forms the total; the shot mean divides by the global shot count, as
+the reference wrapper does. No data-path collective runs inside a time step.
+"""
+import numpy as np
+
+
+def shard(n_items, world, rank):
+    """Round-robin shard of item indices for one rank."""
+    if not (0 <= rank < world):
+        raise ValueError(f"rank {rank} outside world of size {world}")
+    return list(range(rank, n_items, world))
+
+
+def allreduce_sum_(tensors, group=None):
+    """In-place sum over ranks of each torch tensor (any backend)."""
+    import torch.distributed as dist
+    for t in tensors:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return tensors
+
+
+def distributed_gradient(shot_gradient, n_shots, rank, world, shape, group=None, device="cpu"):
+    """Shot-mean gradient and summed misfit over all ranks.
+
+    shot_gradient(s) -> (grad [shape] array-like, misfit float) computes one
+    shot on this rank's device. Returns (grad_mean, misfit_sum) as numpy on
+    every rank."""
+    import torch
+    g = torch.zeros(shape, dtype=torch.float64, device=device)
+    m = torch.zeros(1, dtype=torch.float64, device=device)
+    for s in shard(n_shots, world, rank):
+        gs, ms = shot_gradient(s)
+        g += torch.as_tensor(np.asarray(gs), dtype=torch.float64, device=device)
+        m += float(ms)
+    allreduce_sum_([g, m], group=group)
+    return (g / n_shots).cpu().numpy(), float(m.item())
