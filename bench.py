@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=int(os.environ.get("OTFWI_BENCH_PRECISION", "1")))
     ap.add_argument("--tile", type=int, default=int(os.environ.get("OTFWI_BENCH_TILE", "0")))
+    ap.add_argument("--kernel", type=int, default=int(os.environ.get("OTFWI_BENCH_KERNEL", "-1")),
+                    help="-1 automatic, 0 per-tile, 1 persistent TMA, 2 persistent strip-split")
     ap.add_argument("--X", type=int, default=512)
     ap.add_argument("--T", type=int, default=4000)
     ap.add_argument("--shots", type=int, default=64)
@@ -180,7 +182,7 @@ def run_ours(args):
     from otfwi_b200.distributed import allreduce_sum_
     sc = workload(args, rank)
     b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, prec_deriv=4,
-                  precision=args.precision, tile=args.tile)
+                  precision=args.precision, tile=args.tile, kernel=args.kernel)
     dev = torch.device("cuda", local)
     stream = torch.cuda.ExternalStream(b.stream(), device=dev)
     c_true = torch.tensor(sc.c_true, dtype=torch.float32, device=dev)

@@ -96,7 +96,7 @@ class ShotBatch:
 
     def __init__(self, X, Z, T, PML_size, src_mask, rec_mask, source, prec_deriv=4, shots=None,
                  max_shots=None, precision=0, tile=0, constvec=(1.0, 1.0, 1.0), d_x=None, d_z=None,
-                 kernel=1, lib=None):
+                 kernel=-1, lib=None):
         self._lib = _declare(_lib.load(lib))
         self.X, self.Z, self.T, self.PML = X, Z, T, PML_size
         pz, px = np.where(src_mask)
@@ -170,7 +170,8 @@ class ShotBatch:
         self._ok(self._lib.otf_batch_set_tile(self._h, tile))
 
     def set_kernel(self, variant):
-        """0: one tile per CTA per step; 1: persistent TMA-pipelined CTAs."""
+        """-1: automatic; 0: one tile per CTA per step; 1: persistent
+        TMA-pipelined CTAs; 2: persistent strip-split kernels (fast numerics)."""
         self._ok(self._lib.otf_batch_set_kernel(self._h, variant))
 
     def sync(self):

@@ -114,6 +114,12 @@ struct KernelSet {
     void (*rev_tma)(const TmaParams);
     size_t smem_fwd_tma, smem_rev_tma;
     int grid_fwd_tma, grid_rev_tma;  // persistent grid sizes (set with the attributes)
+    // v3: strip-split kernels (fast numerics only; null when not compiled)
+    void (*fwd_split)(const TmaParams);
+    void (*fwd_ring_split)(const TmaParams);
+    void (*rev_split)(const TmaParams);
+    size_t smem_fwd_split, smem_rev_split;
+    int grid_fwd_split, grid_rev_split, nth_split;
 };
 
 template <int TX, int TZ, class Prec, bool SEP>
@@ -139,6 +145,18 @@ static KernelSet make_set_tma()
     return k;
 }
 
+template <int TX, int TZ, int BH, int NTH, int MINB>
+static void add_split(KernelSet &k)
+{
+    using G = SplitGeom<TX, TZ, BH, NTH>;
+    k.fwd_split = k_forward_split<TX, TZ, BH, NTH, false, MINB>;
+    k.fwd_ring_split = k_forward_split<TX, TZ, BH, NTH, true, MINB>;
+    k.rev_split = k_reverse_split<TX, TZ, BH, NTH, MINB>;
+    k.smem_fwd_split = G::FWD_BYTES;
+    k.smem_rev_split = G::REV_BYTES;
+    k.nth_split = NTH;
+}
+
 struct KernelTable {
     KernelSet s[kNumTileShapes][2][2];  // [shape][precision][separable]
     bool attrs_set = false;
@@ -155,6 +173,9 @@ struct KernelTable {
         s[3][kFast][1] = make_set<248, 24, Fast, true>();
         s[4][kFaithful][1] = make_set_tma<56, 24, Faithful, true, 2>();
         s[4][kFast][1] = make_set_tma<56, 24, Fast, true, 2>();
+        add_split<56, 56, 2, 512, 1>(s[0][kFast][1]);
+        add_split<120, 24, 2, 512, 1>(s[1][kFast][1]);
+        add_split<56, 24, 2, 256, 2>(s[4][kFast][1]);
         // general (non-separable) damping: compiled for the first shape only
         s[0][kFaithful][0] = make_set_tma<56, 56, Faithful, false, 1>();
         s[0][kFast][0] = make_set_tma<56, 56, Fast, false, 1>();
@@ -194,6 +215,25 @@ struct KernelTable {
                     OTF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.rev_tma, NT, k.smem_rev_tma));
                     OTF_CHECK(nb >= 1, 4, "persistent reverse kernel does not fit on an SM");
                     k.grid_rev_tma = nb * nsm;
+                    if (!k.fwd_split)
+                        continue;
+                    void (*fs[2])(const TmaParams) = {k.fwd_split, k.fwd_ring_split};
+                    for (auto f : fs) {
+                        OTF_CUDA(cudaFuncSetAttribute((const void *)f,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)k.smem_fwd_split));
+                        OTF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, k.nth_split,
+                                                                               k.smem_fwd_split));
+                        OTF_CHECK(nb >= 1, 4, "strip-split forward kernel does not fit on an SM");
+                        k.grid_fwd_split = nb * nsm;
+                    }
+                    OTF_CUDA(cudaFuncSetAttribute((const void *)k.rev_split,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)k.smem_rev_split));
+                    OTF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.rev_split, k.nth_split,
+                                                                           k.smem_rev_split));
+                    OTF_CHECK(nb >= 1, 4, "strip-split reverse kernel does not fit on an SM");
+                    k.grid_rev_split = nb * nsm;
                 }
         attrs_set = true;
         return 0;
@@ -329,6 +369,8 @@ int Engine::init(const EngineConfig &cfg, const float *d_x, const float *d_z)
         OTF_CUDA(cudaMalloc(&dampz_, sizeof(float) * L_.rows));
         OTF_CUDA(cudaMemcpy(dampx_, hx.data(), sizeof(float) * L_.pitch, cudaMemcpyHostToDevice));
         OTF_CUDA(cudaMemcpy(dampz_, hz.data(), sizeof(float) * L_.rows, cudaMemcpyHostToDevice));
+        hdampx_ = hx;
+        hdampz_ = hz;
     } else {
         std::vector<float> hx(L_.slot, 1.f), hz(L_.slot, 1.f);
         for (int z = 0; z < Z; z++)
@@ -531,15 +573,21 @@ int Engine::set_shots(int n_shots, const int *ptr, const int *srcs)
 
     // forward injection CSR in a fixed layout (so captured graphs stay valid
     // when only the firing pattern changes): ptr[max_shots+1] | x[cap] | z[cap] | row[cap]
+    // ... | fire[max_shots][n_src]: source k's running-integral row in shot s, -1 if silent
     const size_t np = (size_t)cfg_.max_shots + 1;
-    std::vector<int> h(np + 3 * cap, 0);
+    const size_t nf = (size_t)cfg_.max_shots * std::max(n_src_, 1);
+    std::vector<int> h(np + 3 * cap + nf, 0);
     std::copy(shot_ptr_.begin(), shot_ptr_.end(), h.begin());
-    int *hx = h.data() + np, *hz = hx + cap, *hr = hz + cap;
+    int *hx = h.data() + np, *hz = hx + cap, *hr = hz + cap, *hf = hr + cap;
     for (size_t k = 0; k < shot_srcs_.size(); k++) {
         hx[k] = src_x_[shot_srcs_[k]];
         hz[k] = src_z_[shot_srcs_[k]];
         hr[k] = shot_srcs_[k];
     }
+    std::fill(hf, hf + nf, -1);
+    for (int s = 0; s < n_shots; s++)
+        for (int k = shot_ptr_[s]; k < shot_ptr_[s + 1]; k++)
+            hf[(size_t)s * std::max(n_src_, 1) + shot_srcs_[k]] = shot_srcs_[k];
     if (h.size() != inj_src_cap_) {
         if (inj_src_)
             cudaFree(inj_src_);
@@ -554,6 +602,7 @@ int Engine::set_shots(int n_shots, const int *ptr, const int *srcs)
     inj_src_x_ = inj_src_ + np;
     inj_src_z_ = inj_src_x_ + cap;
     inj_src_row_ = inj_src_z_ + cap;
+    fire_row_ = inj_src_row_ + cap;
     return 0;
 }
 
@@ -623,6 +672,39 @@ int Engine::build_tables()
     const size_t o_ringe = h.size();
     flatten(ringe, true, dummy);
 
+    // points inside each tile's halo-extended region (strip-split kernels):
+    // sources (the shot's firing table decides whether they fire) and the
+    // receivers that take adjoint injection
+    auto in_regions = [&](int x, int z, int id, std::vector<std::vector<std::pair<int, int>>> &v) {
+        for (int tz = std::max(0, (z - 4) / TZ - 1); tz <= std::min(ntz - 1, (z + 4) / TZ + 1); tz++)
+            for (int tx = std::max(0, (x - 4) / TX - 1); tx <= std::min(ntx - 1, (x + 4) / TX + 1); tx++) {
+                const int ex = x - (tx * TX - 4), ez = z - (tz * TZ - 4);
+                if (ex >= 0 && ex < EX && ez >= 0 && ez < TZ + 8)
+                    v[tz * ntx + tx].push_back({ez * EX + ex, id});
+            }
+    };
+    std::vector<std::vector<std::pair<int, int>>> srce(ntiles), rcve(ntiles);
+    for (int k = 0; k < n_src_; k++)
+        in_regions(src_x_[k], src_z_[k], k, srce);
+    for (int n = 0; n < n_rec_; n++)
+        if (interior(rec_x_[n], rec_z_[n], X, Z))
+            in_regions(rec_x_[n], rec_z_[n], n, rcve);
+    const size_t o_srce = h.size();
+    flatten(srce, true, dummy);
+    const size_t o_rcve = h.size();
+    flatten(rcve, true, dummy);
+    // tiles whose region holds a damped or never-updated cell
+    const size_t o_edge = h.size();
+    for (int tl = 0; tl < ntiles; tl++) {
+        const int x0 = (tl % ntx) * TX, z0 = (tl / ntx) * TZ;
+        bool edge = !sep_ || x0 - 4 < 4 || z0 - 4 < 4 || x0 + TX + 4 > X - 4 || z0 + TZ + 4 > Z - 4;
+        for (int x = std::max(0, x0 - 4); !edge && x < std::min(X, x0 + TX + 4); x++)
+            edge = hdampx_[x + PAD] != 1.f;
+        for (int z = std::max(0, z0 - 4); !edge && z < std::min(Z, z0 + TZ + 4); z++)
+            edge = hdampz_[z + PAD] != 1.f;
+        h.push_back(edge ? 1 : 0);
+    }
+
     // adjoint injection: every receiver of shot s with tab row s*n_rec + n
     const size_t o_adj = h.size();
     {
@@ -666,6 +748,21 @@ int Engine::build_tables()
     inj_adj_x_ = inj_adj_ptr_ + n_shots_ + 1;
     inj_adj_z_ = inj_adj_x_ + n_rec_ * n_shots_;
     inj_adj_row_ = inj_adj_z_ + n_rec_ * n_shots_;
+    srce_ptr_ = d + o_srce;
+    srce_cell_ = srce_ptr_ + ntiles + 1;
+    {
+        int ne = 0;
+        for (auto &v : srce)
+            ne += (int)v.size();
+        srce_id_ = srce_cell_ + ne + 1;
+        ne = 0;
+        for (auto &v : rcve)
+            ne += (int)v.size();
+        rcve_ptr_ = d + o_rcve;
+        rcve_cell_ = rcve_ptr_ + ntiles + 1;
+        rcve_id_ = rcve_cell_ + ne + 1;
+    }
+    tile_edge_ = d + o_edge;
     tables_dirty_ = false;
     drop_graphs();
     return 0;
@@ -701,21 +798,43 @@ StepParams Engine::base_params() const
     p.ring = ring_;
     p.n_ring = n_ring_;
     p.grad = grad_;
+    p.tile_edge = tile_edge_;
+    p.srce_ptr = srce_ptr_;
+    p.srce_cell = srce_cell_;
+    p.srce_id = srce_id_;
+    p.fire_row = fire_row_;
+    p.n_src = std::max(n_src_, 1);
+    p.rcve_ptr = rcve_ptr_;
+    p.rcve_cell = rcve_cell_;
+    p.rcve_id = rcve_id_;
     return p;
 }
 
-bool use_tma(const KernelSet &k, int variant) { return variant == 1 && k.fwd_tma != nullptr; }
+// Kernel variant actually used: the requested one where compiled for the
+// tile shape and numerics, else the next simpler one (2 -> 1 -> 0). The
+// strip-split kernels (2) implement the fast numerics only; -1 = automatic
+// (2 for fast, 1 for faithful).
+static int resolve_variant(const KernelSet &k, int requested, int precision)
+{
+    int v = requested < 0 ? (precision == kFast ? 2 : 1) : requested;
+    if (v == 2 && !(precision == kFast && k.fwd_split))
+        v = 1;
+    if (v == 1 && !k.fwd_tma)
+        v = 0;
+    return v;
+}
 
 int Engine::variant_in_use() const
 {
-    return use_tma(ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0], variant_) ? 1 : 0;
+    return resolve_variant(ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0], variant_, cfg_.precision);
 }
 
 // One forward step launch. pin / ain: slots holding P(t-1) / A(t-1).
 int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, int pin, int ain)
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
-    if (use_tma(k, variant_)) {
+    const int v = resolve_variant(k, variant_, cfg_.precision);
+    if (v >= 1) {
         TmaParams P = *tmap_;
         P.p = p;
         P.s0_p_in = pin;
@@ -725,9 +844,14 @@ int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, 
         P.n_items = (int)(grid.x * grid.y);
         P.err = derr_;
         void *args[] = {(void *)&P};
-        OTF_CUDA(cudaLaunchKernel((const void *)(with_ring ? k.fwd_ring_tma : k.fwd_tma),
-                                  dim3(std::min(k.grid_fwd_tma, P.n_items)), dim3(NT), args,
-                                  k.smem_fwd_tma, st_));
+        if (v == 2)
+            OTF_CUDA(cudaLaunchKernel((const void *)(with_ring ? k.fwd_ring_split : k.fwd_split),
+                                      dim3(std::min(k.grid_fwd_split, P.n_items)), dim3(k.nth_split),
+                                      args, k.smem_fwd_split, st_));
+        else
+            OTF_CUDA(cudaLaunchKernel((const void *)(with_ring ? k.fwd_ring_tma : k.fwd_tma),
+                                      dim3(std::min(k.grid_fwd_tma, P.n_items)), dim3(NT), args,
+                                      k.smem_fwd_tma, st_));
         return 0;
     }
     void *args[] = {(void *)&p};
@@ -740,7 +864,8 @@ int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, 
 int Engine::launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain, int in1)
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
-    if (use_tma(k, variant_)) {
+    const int v = resolve_variant(k, variant_, cfg_.precision);
+    if (v >= 1) {
         TmaParams P = *tmap_;
         P.p = p;
         P.s0_p_in = pin;
@@ -750,8 +875,13 @@ int Engine::launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain
         P.n_items = (int)(grid.x * grid.y);
         P.err = derr_;
         void *args[] = {(void *)&P};
-        OTF_CUDA(cudaLaunchKernel((const void *)k.rev_tma, dim3(std::min(k.grid_rev_tma, P.n_items)),
-                                  dim3(NT), args, k.smem_rev_tma, st_));
+        if (v == 2)
+            OTF_CUDA(cudaLaunchKernel((const void *)k.rev_split,
+                                      dim3(std::min(k.grid_rev_split, P.n_items)), dim3(k.nth_split),
+                                      args, k.smem_rev_split, st_));
+        else
+            OTF_CUDA(cudaLaunchKernel((const void *)k.rev_tma, dim3(std::min(k.grid_rev_tma, P.n_items)),
+                                      dim3(NT), args, k.smem_rev_tma, st_));
         return 0;
     }
     void *args[] = {(void *)&p};
@@ -788,7 +918,7 @@ int Engine::build_maps()
 
 int Engine::set_variant(int variant)
 {
-    OTF_CHECK(variant == 0 || variant == 1, 1, "unknown kernel variant");
+    OTF_CHECK(variant >= -1 && variant <= 2, 1, "unknown kernel variant");
     if (variant != variant_) {
         variant_ = variant;
         drop_graphs();
@@ -898,7 +1028,7 @@ int Engine::prepare()
     OTF_CHECK(!shot_ptr_.empty(), 2, "no shots configured");
     if (tables_dirty_ && build_tables())
         return -1;
-    if (variant_in_use() == 1 && maps_dirty_ && build_maps())
+    if (variant_in_use() >= 1 && maps_dirty_ && build_maps())
         return -1;
     return 0;
 }

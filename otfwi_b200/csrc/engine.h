@@ -7,6 +7,7 @@
 #include "otf_common.cuh"
 #include "pml_step.cuh"
 #include "pml_step_tma.cuh"
+#include "pml_step_split.cuh"
 
 namespace otf {
 
@@ -78,8 +79,8 @@ class Engine {
     const Layout &layout() const { return L_; }
     int set_precision(int prec);
     int set_tile(int tile);
-    // 0: one tile per CTA; 1: persistent TMA-pipelined kernels where the tile
-    // shape supports them (default)
+    // -1 automatic (default); 0 one tile per CTA; 1 persistent TMA-pipelined;
+    // 2 persistent strip-split (fast numerics). Falls back where not compiled.
     int set_variant(int variant);
     int variant_in_use() const;
     // waits for the stream and reports a timed-out bounded wait in a kernel
@@ -140,7 +141,13 @@ class Engine {
     int graph_shots_ = -1;
     bool tables_dirty_ = true;
 
-    int variant_ = 1;
+    // strip-split (fast) kernel tables
+    int *srce_ptr_ = nullptr, *srce_cell_ = nullptr, *srce_id_ = nullptr;
+    int *rcve_ptr_ = nullptr, *rcve_cell_ = nullptr, *rcve_id_ = nullptr;
+    int *tile_edge_ = nullptr, *fire_row_ = nullptr;
+    std::vector<float> hdampx_, hdampz_;  // host copies of the separable multipliers (padded index)
+
+    int variant_ = -1;
     int *derr_ = nullptr;         // device error flag of the bounded waits
     TmaParams *tmap_ = nullptr;   // tensor maps of every field, slot and coefficient
     bool maps_dirty_ = true;

@@ -135,6 +135,14 @@ struct StepParams {
     float *ring;  // [n_shots][T][n_ring]
     int n_ring;
     float *grad;  // padded [n_shots][rows][pitch]
+    // strip-split (fast) kernels: per-tile flag (1 = the tile's halo region
+    // holds damped or never-updated cells), per-tile point lists over the
+    // halo region, and the firing table of sources per shot
+    const int *tile_edge;                     // [ntiles]
+    const int *srce_ptr, *srce_cell, *srce_id;  // sources in each tile's region
+    const int *fire_row;                      // [n_shots][n_src]: tab row, -1 = silent
+    int n_src;
+    const int *rcve_ptr, *rcve_cell, *rcve_id;  // injectable receivers in each region
 };
 
 template <int TX, int TZ>

@@ -113,6 +113,36 @@ def test_persistent_tma_kernels_bit_identical_to_per_tile(lib, tile, precision):
         assert np.array_equal(a[k], b[k]), (tile, precision, k)
 
 
+def _strip_case():
+    """Sources and receivers inside the damped strips (the split component
+    Q is injected into and recorded from there)."""
+    import make_sim_golden
+    from otfwi_b200 import scenarios
+    from otfwi_b200.cuda_interface_pml import pml_damping
+    sc = scenarios.small(X=112, Z=90, T=260, n_src=2, n_rec=6, seed=9, f0=0.05)
+    sc.src_mask[:] = False
+    sc.src_mask[10, 30] = True   # inside the top strip
+    sc.src_mask[50, 8] = True    # inside the left strip
+    sc.rec_mask[:] = False
+    sc.rec_mask[12, [20, 50, 80]] = True
+    sc.rec_mask[[40, 60], 104] = True
+    sc.rec_mask[86, 60] = True   # within 4 cells of the edge: records zeros
+    return make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))
+
+
+@pytest.mark.parametrize("tile", [0, 1, 4])
+def test_strip_split_kernels_close_to_oracle(lib, tile):
+    """Fast numerics with P everywhere and the split component only on damped
+    cells: within the fast-mode tolerance of the FP64 oracle and of the
+    split-field fast kernels, on the medium case and on a case with sources
+    and receivers inside the strips."""
+    for inp in (_cases()["medium"], _strip_case()):
+        res = _run(lib, inp, precision=1, tile=tile, kernel=2)
+        _assert_close(res, oracle_case(inp, "f64"), 1e-4, 1e-3, f"split vs oracle f64 tile {tile}")
+        ref = _run(lib, inp, precision=1, tile=tile, kernel=1)
+        _assert_close(res, ref, 1e-4, 1e-3, f"split vs split-field fast tile {tile}")
+
+
 def test_odd_grid_sizes_every_tile(lib):
     """Grids that are not multiples of any tile shape, both kernel variants."""
     import make_sim_golden
@@ -124,6 +154,10 @@ def test_odd_grid_sizes_every_tile(lib):
     for tile in range(5):
         for kernel in (0, 1):
             _assert_identical(_run(lib, inp, tile=tile, kernel=kernel), ref, f"odd grid tile {tile} k{kernel}")
+    ref64 = oracle_case(inp, "f64")
+    for tile in (0, 1, 4):
+        _assert_close(_run(lib, inp, precision=1, tile=tile, kernel=2), ref64, 1e-4, 1e-3,
+                      f"odd grid split tile {tile}")
 
 
 def test_edge_receiver_records_zero(lib):
