@@ -45,7 +45,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=int(os.environ.get("OTFWI_BENCH_PRECISION", "1")))
-    ap.add_argument("--tile", type=int, default=int(os.environ.get("OTFWI_BENCH_TILE", "0")))
+    ap.add_argument("--tile", type=int, default=int(os.environ.get("OTFWI_BENCH_TILE", "-1")),
+                    help="tile shape index; -1 = chosen by the autotuner (otfwi_b200.autotune)")
     ap.add_argument("--kernel", type=int, default=int(os.environ.get("OTFWI_BENCH_KERNEL", "-1")),
                     help="-1 automatic, 0 per-tile, 1 persistent TMA, 2 persistent strip-split")
     ap.add_argument("--X", type=int, default=512)
@@ -181,6 +182,14 @@ def run_ours(args):
     from otfwi_b200.batch import ShotBatch
     from otfwi_b200.distributed import allreduce_sum_
     sc = workload(args, rank)
+    tuned = None
+    if args.tile < 0:
+        from otfwi_b200.autotune import autotune, TILES
+        k, t, table = autotune(sc, precision=args.precision, misfit=args.misfit)
+        if args.kernel < 0:
+            args.kernel = k
+        args.tile = t
+        tuned = {"kernel": k, "tile": list(TILES[t]), "candidates_ms_T300": table}
     b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, prec_deriv=4,
                   precision=args.precision, tile=args.tile, kernel=args.kernel)
     dev = torch.device("cuda", local)
@@ -298,7 +307,8 @@ def run_ours(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded model, Ricker source; no external dataset)",
-                "config": config_block(args, sc, f"shots-per-rank, gradient all-reduce, {world} rank(s)"),
+                "config": dict(config_block(args, sc, f"shots-per-rank, gradient all-reduce, {world} rank(s)"),
+                               kernel_variant=args.kernel, tile=args.tile, autotune=tuned),
                 "roofline": roof, "e2e": e2e,
                 # per step: T-1 forward + T-1 reverse step kernels, misfit,
                 # misfit sum, adjoint running integral, shot mean

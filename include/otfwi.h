@@ -141,8 +141,31 @@ int otf_batch_adjoint(otf_batch *b, float *adj, int on_device);  /* copy out the
 int otf_batch_reverse(otf_batch *b, const float *adj, int on_device, float *grad, float scale,
                       int grad_on_device);
 int otf_batch_shot_grad(otf_batch *b, int shot, float *grad, int on_device); /* one shot's [Z*X] */
+/* Differentiable forward: traces of every shot while keeping the full
+ * wavefield every `every` steps (sqrt(T) is the memory optimum). */
+int otf_batch_forward_ckpt(otf_batch *b, int every, float *traces, int on_device);
+/* Exact discrete adjoint of the last otf_batch_forward_ckpt:
+ * grad_c2 [Z*X] = sum over shots of dL/d(c^2) for dL/dtraces = g
+ * [n_shots][n_rec][T]. Each checkpoint segment's forward is recomputed once.
+ * No reference counterpart: the reference's gradient (cuda_grad_ext)
+ * cross-correlates a reconstructed field, an approximation of this one. */
+int otf_batch_backward_exact(otf_batch *b, const float *g, int g_on_device, float *grad_c2,
+                             int grad_on_device);
 int otf_batch_sync(otf_batch *b);
 void *otf_batch_stream(otf_batch *b);
+/* Results of the last gradient of this batch (also after otf_multi_gradient). */
+int otf_batch_last_gradient(otf_batch *b, float *grad, double *misfit, int on_device);
+
+/* Several independent inversions -- different grids, shot counts and T --
+ * as parallel branches of one CUDA graph: otf_multi_gradient computes every
+ * instance's gradient in one graph launch; after otf_multi_sync read each
+ * with otf_batch_last_gradient. The instances stay owned by the caller and
+ * must outlive the group. No reference counterpart. */
+typedef struct otf_multi otf_multi;
+otf_multi *otf_multi_create(int n, otf_batch **batches);
+void otf_multi_destroy(otf_multi *m);
+int otf_multi_gradient(otf_multi *m, int misfit_kind);
+int otf_multi_sync(otf_multi *m);
 
 /* Stand-alone device misfit over n_traces traces [n_traces][T] (device
  * pointers, misfit [n_traces] FP64) with caller-owned scratch of at least

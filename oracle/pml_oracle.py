@@ -37,11 +37,53 @@ def _load():
     lib.orc_simulate_f64.argtypes = common + [dp]
     lib.orc_grad_f32.argtypes = common + [c_int, ip, ip, _cbf, c_void_p, fp, fp]
     lib.orc_grad_f64.argtypes = common + [c_int, ip, ip, _cbd, c_void_p, dp, dp]
+    lib.orc_exact_adjoint_f64.argtypes = common + [dp, dp, dp]
+    lib.orc_forward_f64.argtypes = [c_int, c_int, c_int, dp, fp, fp, fp, c_int, ip, ip, fp, c_int, c_int,
+                                    ip, ip, dp]
     for f in (lib.orc_simulate_f32, lib.orc_simulate_f64, lib.orc_grad_f32, lib.orc_grad_f64,
-              lib.orc_num_threads):
+              lib.orc_num_threads, lib.orc_exact_adjoint_f64, lib.orc_forward_f64):
         f.restype = c_int
     _lib = lib
     return lib
+
+
+def exact_adjoint(cquad, constvec, d_x, d_z, src_x, src_z, source, rec_x, rec_z, g, idx_source=-1):
+    """(dL/d(c^2) [Z, X], traces [n_rec, T]) of the exact discrete adjoint
+    (oracle/pml_adjoint.c) for dL/drec = g [n_rec, T], FP64."""
+    lib = _load()
+    Z, X = np.asarray(cquad).shape
+    nsrc = len(np.atleast_1d(src_x))
+    T = np.asarray(source).reshape(nsrc, -1).shape[1]
+    arrs = _prep(cquad, constvec, d_x, d_z, src_x, src_z, source, rec_x, rec_z)
+    nm = len(arrs[7])
+    gg = np.ascontiguousarray(np.asarray(g, dtype=np.float64).reshape(nm, T))
+    grad = np.zeros((Z, X))
+    rec = np.zeros((nm, T))
+    dp = POINTER(c_double)
+    rc = lib.orc_exact_adjoint_f64(*_args(X, Z, T, arrs, idx_source), gg.ctypes.data_as(dp),
+                                   grad.ctypes.data_as(dp), rec.ctypes.data_as(dp))
+    if rc:
+        raise RuntimeError("oracle exact adjoint failed")
+    return grad, rec
+
+
+def forward64(cquad64, constvec, d_x, d_z, src_x, src_z, source, rec_x, rec_z, idx_source=-1):
+    """FP64 traces [n_rec, T] of the same map, with an FP64 c^2 (for finite
+    differences)."""
+    lib = _load()
+    cq = np.ascontiguousarray(np.asarray(cquad64, dtype=np.float64))
+    Z, X = cq.shape
+    nsrc = len(np.atleast_1d(src_x))
+    T = np.asarray(source).reshape(nsrc, -1).shape[1]
+    arrs = _prep(cq, constvec, d_x, d_z, src_x, src_z, source, rec_x, rec_z)
+    nm = len(arrs[7])
+    rec = np.zeros((nm, T))
+    a = _args(X, Z, T, arrs, idx_source)
+    a[3] = cq.ctypes.data_as(POINTER(c_double))
+    rc = lib.orc_forward_f64(*a, rec.ctypes.data_as(POINTER(c_double)))
+    if rc:
+        raise RuntimeError("oracle forward failed")
+    return rec
 
 
 def num_threads():

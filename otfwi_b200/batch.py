@@ -257,3 +257,61 @@ def device_misfit(sim, obs, misfit="wasserstein", lib=None):
         raise _lib.OtfwiError("otf_misfit failed")
     torch.cuda.synchronize()
     return mis.cpu().numpy(), adj.cpu().numpy()
+
+
+class MultiBatch:
+    """Independent inversions (different grids, shot counts and T) whose
+    gradients run as parallel branches of one CUDA graph (otf_multi_*): one
+    launch for all of them. The ShotBatch instances stay owned by the caller."""
+
+    def __init__(self, batches):
+        self.batches = list(batches)
+        L = self._lib = self.batches[0]._lib
+        if not getattr(L, "_multi_declared", False):
+            L.otf_multi_create.restype = c_void_p
+            L.otf_multi_create.argtypes = [c_int, ctypes.c_void_p]
+            L.otf_multi_destroy.restype = None
+            L.otf_multi_destroy.argtypes = [c_void_p]
+            for name in ("otf_multi_gradient",):
+                getattr(L, name).restype = c_int
+                getattr(L, name).argtypes = [c_void_p, c_int]
+            L.otf_multi_sync.restype = c_int
+            L.otf_multi_sync.argtypes = [c_void_p]
+            L.otf_batch_last_gradient.restype = c_int
+            L.otf_batch_last_gradient.argtypes = [c_void_p, c_void_p, c_void_p, c_int]
+            L._multi_declared = True
+        arr = (c_void_p * len(self.batches))(*[b._h.value for b in self.batches])
+        h = L.otf_multi_create(len(self.batches), arr)
+        if not h:
+            _lib.check(L)
+            raise _lib.OtfwiError("otf_multi_create failed")
+        self._h = c_void_p(h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.otf_multi_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def gradient(self, misfit="wasserstein"):
+        """[(grad [Z, X], misfit)] of every instance from one graph launch."""
+        kind = MISFITS[misfit] if isinstance(misfit, str) else int(misfit)
+        L = self._lib
+        for rc in (L.otf_multi_gradient(self._h, kind), L.otf_multi_sync(self._h)):
+            if rc != 0:
+                _lib.check(L)
+                raise _lib.OtfwiError("multi-instance gradient failed")
+        out = []
+        for b in self.batches:
+            g = np.zeros((b.Z, b.X), np.float32)
+            m = np.zeros(1, np.float64)
+            b._ok(L.otf_batch_last_gradient(b._h, ctypes.c_void_p(g.ctypes.data),
+                                            ctypes.c_void_p(m.ctypes.data), 0))
+            b.sync()
+            out.append((g, float(m[0])))
+        return out

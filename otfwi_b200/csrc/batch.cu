@@ -6,6 +6,7 @@
 // the misfit on the host (adjoint_functions.py).
 #include <cuda_runtime.h>
 #include <memory>
+#include <vector>
 #include "engine.h"
 #include "misfit.h"
 #include "../../include/otfwi.h"
@@ -146,7 +147,132 @@ int otf_batch_adjoint(otf_batch *b, float *adj, int on_device)
     return 0;
 }
 
+int otf_batch_forward_ckpt(otf_batch *b, int every, float *traces, int on_device)
+{
+    if (b->eng.forward_checkpointed(every))
+        return -1;
+    if (traces && b->eng.copy_traces(traces, 0, b->eng.n_shots(), kind_out(on_device)))
+        return -1;
+    return 0;
+}
+
+int otf_batch_backward_exact(otf_batch *b, const float *g, int g_on_device, float *grad_c2,
+                             int grad_on_device)
+{
+    const otf::EngineConfig &c = b->eng.config();
+    const size_t ng = (size_t)b->eng.n_shots() * b->eng.n_rec() * c.T, nz = (size_t)c.X * c.Z;
+    float *gd = const_cast<float *>(g), *out = grad_c2;
+    cudaStream_t st = b->eng.stream();
+    if (!g_on_device) {
+        OTF_CUDA(cudaMallocAsync(&gd, sizeof(float) * ng, st));
+        OTF_CUDA(cudaMemcpyAsync(gd, g, sizeof(float) * ng, cudaMemcpyHostToDevice, st));
+    }
+    if (!grad_on_device)
+        OTF_CUDA(cudaMallocAsync(&out, sizeof(float) * nz, st));
+    const int rc = b->eng.backward_exact(gd, out);
+    if (!rc && !grad_on_device)
+        OTF_CUDA(cudaMemcpyAsync(grad_c2, out, sizeof(float) * nz, cudaMemcpyDeviceToHost, st));
+    if (!g_on_device)
+        cudaFreeAsync(gd, st);
+    if (!grad_on_device)
+        cudaFreeAsync(out, st);
+    return rc;
+}
+
 int otf_batch_sync(otf_batch *b) { return b->eng.sync(); }
+
+int otf_batch_last_gradient(otf_batch *b, float *grad, double *misfit, int on_device)
+{
+    const otf::EngineConfig &c = b->eng.config();
+    OTF_CHECK(b->eng.grad_mean_dev() != nullptr, 2, "no gradient has been computed on this batch");
+    if (grad)
+        OTF_CUDA(cudaMemcpyAsync(grad, b->eng.grad_mean_dev(), sizeof(float) * (size_t)c.X * c.Z,
+                                 kind_out(on_device), b->eng.stream()));
+    if (misfit)
+        OTF_CUDA(cudaMemcpyAsync(misfit, b->eng.misfit_total_dev(), sizeof(double), kind_out(on_device),
+                                 b->eng.stream()));
+    return 0;
+}
+
+}  // extern "C"
+
+// Several independent inversions (different grids, shot counts and T) in one
+// CUDA graph: each instance's complete gradient graph is a parallel branch,
+// so one launch runs them all and the GPU fills its SMs from every branch.
+struct otf_multi {
+    std::vector<otf_batch *> b;
+    cudaStream_t st = nullptr;
+    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+    ~otf_multi()
+    {
+        for (auto &e : exec)
+            if (e)
+                cudaGraphExecDestroy(e);
+        if (st)
+            cudaStreamDestroy(st);
+    }
+};
+
+extern "C" {
+
+otf_multi *otf_multi_create(int n, otf_batch **batches)
+{
+    otf::clear_error();
+    if (n < 1 || !batches) {
+        otf::set_error_msg(1, "otf_multi_create: no instances");
+        return nullptr;
+    }
+    std::unique_ptr<otf_multi> m(new otf_multi());
+    m->b.assign(batches, batches + n);
+    if (cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking) != cudaSuccess) {
+        otf::set_error_msg(2, "otf_multi_create: stream creation failed");
+        return nullptr;
+    }
+    return m.release();
+}
+
+void otf_multi_destroy(otf_multi *m) { delete m; }
+
+int otf_multi_gradient(otf_multi *m, int misfit_kind)
+{
+    OTF_CHECK(misfit_kind >= 0 && misfit_kind < 3, 1, "unknown misfit kind");
+    if (!m->exec[misfit_kind]) {
+        cudaGraph_t parent = nullptr;
+        OTF_CUDA(cudaGraphCreate(&parent, 0));
+        for (otf_batch *b : m->b) {
+            cudaGraph_t child = nullptr;
+            if (b->eng.gradient_graph(misfit_kind, &child)) {
+                cudaGraphDestroy(parent);
+                return -1;
+            }
+            cudaGraphNode_t node;
+            const cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
+            cudaGraphDestroy(child);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(parent);
+                OTF_CUDA(e);
+            }
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&m->exec[misfit_kind], parent, 0);
+        cudaGraphDestroy(parent);
+        OTF_CUDA(ei);
+    }
+    // every instance's own stream work (model / observed uploads) precedes the launch
+    for (otf_batch *b : m->b)
+        if (b->eng.sync())
+            return -1;
+    OTF_CUDA(cudaGraphLaunch(m->exec[misfit_kind], m->st));
+    return 0;
+}
+
+int otf_multi_sync(otf_multi *m)
+{
+    OTF_CUDA(cudaStreamSynchronize(m->st));
+    for (otf_batch *b : m->b)
+        if (b->eng.sync())  // surfaces a device-side wait timeout of any instance
+            return -1;
+    return 0;
+}
 
 void *otf_batch_stream(otf_batch *b) { return (void *)b->eng.stream(); }
 

@@ -323,6 +323,13 @@ void Engine::free_all()
     if (derr_)
         cudaFree(derr_);
     derr_ = nullptr;
+    if (ckpt_)
+        cudaFree(ckpt_);
+    if (seg_)
+        cudaFree(seg_);
+    ckpt_ = seg_ = nullptr;
+    ckpt_bytes_ = seg_bytes_ = 0;
+    ck_valid_ = false;
     delete tmap_;
     tmap_ = nullptr;
     maps_dirty_ = true;
@@ -1057,7 +1064,9 @@ int Engine::reverse()
 // The whole multi-shot gradient as one graph: forward with ring recording,
 // device misfit and adjoint sources, reverse phase, and the shot mean of the
 // gradients into grad_mean_dev() / the misfit total into misfit_total_dev().
-int Engine::gradient(int kind)
+// Buffers the gradient graph writes outside the per-step state; allocated
+// before any capture (no allocation inside a graph).
+int Engine::prepare_gradient(int kind)
 {
     if (prepare())
         return -1;
@@ -1066,7 +1075,6 @@ int Engine::gradient(int kind)
         OTF_CUDA(cudaMalloc(&gsum_, sizeof(float) * (size_t)cfg_.X * cfg_.Z));
         OTF_CUDA(cudaMalloc(&tot_, sizeof(double)));
     }
-    // the misfit scratch must exist before capture (no allocation inside a graph)
     const int64_t need = misfit_scratch_per_trace(kind, cfg_.T) * n_shots_ * n_rec_;
     if (need > mscratch_bytes_) {
         drop_graphs();
@@ -1076,14 +1084,42 @@ int Engine::gradient(int kind)
         OTF_CUDA(cudaMalloc(&mscratch_, (size_t)need));
         mscratch_bytes_ = need;
     }
-    if (!g_grad_[kind] && capture(&g_grad_[kind], [&] {
-            if (emit_forward(true) || misfit(kind, tot_) || emit_reverse() ||
-                grad_sum(gsum_, 0.0f))
-                return -1;
-            return 0;
-        }))
+    return 0;
+}
+
+int Engine::emit_gradient(int kind)
+{
+    if (emit_forward(true) || misfit(kind, tot_) || emit_reverse() || grad_sum(gsum_, 0.0f))
+        return -1;
+    return 0;
+}
+
+int Engine::gradient(int kind)
+{
+    if (prepare_gradient(kind))
+        return -1;
+    if (!g_grad_[kind] && capture(&g_grad_[kind], [&] { return emit_gradient(kind); }))
         return -1;
     OTF_CUDA(cudaGraphLaunch(g_grad_[kind], st_));
+    return 0;
+}
+
+int Engine::gradient_graph(int kind, cudaGraph_t *out)
+{
+    *out = nullptr;
+    if (prepare_gradient(kind))
+        return -1;
+    OTF_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    const int rc = emit_gradient(kind);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(st_, &g);
+    if (rc) {
+        if (g)
+            cudaGraphDestroy(g);
+        return rc;
+    }
+    OTF_CUDA(ec);
+    *out = g;
     return 0;
 }
 

@@ -66,6 +66,17 @@ class Engine {
     int misfit(int kind, double *total_dev);
     // forward + misfit + reverse + shot mean, replayed as one CUDA graph
     int gradient(int kind);
+    // the same work as an uninstantiated graph (caller owns it), for
+    // composing several engines into one launch
+    int gradient_graph(int kind, cudaGraph_t *out);
+
+    // Differentiable path (engine_adjoint.cu): forward of every shot keeping
+    // the full state every `every` steps (sqrt(T) checkpoints), then the
+    // exact discrete adjoint, recomputing each segment's forward states:
+    // grad_c2 [Z*X] (device, unpadded) = sum over shots of dL/d(c^2) for
+    // dL/drec = g [n_shots][n_rec][T] (device).
+    int forward_checkpointed(int every);
+    int backward_exact(const float *g_dev, float *grad_c2_dev);
     float *grad_mean_dev() { return gsum_; }
     double *misfit_total_dev() { return tot_; }
 
@@ -90,6 +101,8 @@ class Engine {
     int build_tables();
     int build_maps();
     int prepare();
+    int prepare_gradient(int kind);
+    int emit_gradient(int kind);
     int emit_forward(bool with_ring);
     int emit_reverse();
     template <class Emit>
@@ -146,6 +159,13 @@ class Engine {
     int *rcve_ptr_ = nullptr, *rcve_cell_ = nullptr, *rcve_id_ = nullptr;
     int *tile_edge_ = nullptr, *fire_row_ = nullptr;
     std::vector<float> hdampx_, hdampz_;  // host copies of the separable multipliers (padded index)
+
+    // differentiable path: checkpoints [n_ck][4 fields][max_shots][slot] and
+    // the recomputed A history of one segment [every][2][max_shots][slot]
+    float *ckpt_ = nullptr, *seg_ = nullptr;
+    size_t ckpt_bytes_ = 0, seg_bytes_ = 0;
+    int ck_every_ = 0, n_ck_ = 0;
+    bool ck_valid_ = false;
 
     int variant_ = -1;
     int *derr_ = nullptr;         // device error flag of the bounded waits

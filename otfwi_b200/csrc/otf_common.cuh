@@ -44,6 +44,8 @@ struct Layout {
 void set_error(int code, const char *what, const char *file, int line);
 void set_error_msg(int code, const std::string &msg);
 void clear_error();
+int last_status();
+const char *last_error();
 
 }  // namespace otf
 
