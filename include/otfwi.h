@@ -153,6 +153,12 @@ int otf_batch_backward_exact(otf_batch *b, const float *g, int g_on_device, floa
                              int grad_on_device);
 int otf_batch_sync(otf_batch *b);
 void *otf_batch_stream(otf_batch *b);
+/* Forward of every shot and the device misfit only (a line-search objective
+ * evaluation): *misfit = sum over every trace. */
+int otf_batch_objective(otf_batch *b, int misfit_kind, double *misfit, int on_device);
+/* Source illumination illum [Z*X] = sum over shots and over every `every`-th
+ * forward step of P^2 (one forward modelling). */
+int otf_batch_illumination(otf_batch *b, int every, float *illum, int on_device);
 /* Results of the last gradient of this batch (also after otf_multi_gradient). */
 int otf_batch_last_gradient(otf_batch *b, float *grad, double *misfit, int on_device);
 
@@ -186,6 +192,49 @@ int otf_misfit(int kind, const float *sim, const float *obs, float *adj, double 
  * so order them on one stream. Inputs and outputs are caller device memory. */
 int otf_misfit_noalloc(int kind, const float *sim, const float *obs, float *adj, double *misfit,
                        int n_traces, int T, void *stream);
+
+/* ---- Part 4: learned gradient preconditioner (additive) -------------------
+ * Kernels of a BF16 U-Net with FP32 accumulation, trained on the GPU. No
+ * reference counterpart: the reference's inversion is plain L-BFGS-B on the
+ * raw gradient (regression.py:82-88). All pointers are device pointers;
+ * activations are [N][H][W][C] BF16 (void *), C a multiple of 16; conv
+ * weights [9][Cout][Cin] BF16 (tap = 3*dy + dx); launches are asynchronous on
+ * `stream` (a cudaStream_t). Return 0, or -1 with otf_last_error set. */
+
+/* 3x3 convolution, zero padding: input channels [0, c0) from src0 and
+ * [c0, c0+c1) from src1 (at half resolution, upsampled nearest, when up1);
+ * out = bias + conv, ReLU if relu; output channels [0, split) go to dst0
+ * ([..][split]) and [split, cout) to dst1 ([..][cout-split]), each zeroed
+ * where its mask (same layout, optional) is <= 0. cout a multiple of 32. */
+int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1, const void *w,
+                     const float *bias, int relu, void *dst0, const void *mask0, void *dst1,
+                     const void *mask1, int split, int cout, int N, int H, int W, void *stream);
+/* dw [9][cout][c0+c1] (FP32) += weight gradient for the pre-activation
+ * gradient dz [N][H][W][cout] of that convolution's inputs. */
+int otf_unet_conv3x3_wgrad(const void *src0, int c0, const void *src1, int c1, int up1, const void *dz,
+                           int cout, float *dw, int N, int H, int W, int sm_count, void *stream);
+int otf_unet_bias_grad(const void *dz, int C, long long npix, float *db, void *stream); /* db += sum_p dz */
+int otf_unet_pool2(const void *x, void *y, int N, int H, int W, int C, void *stream);  /* 2x2 mean */
+/* dx += 0.25 * dy(parent) where x > 0 */
+int otf_unet_pool2_bwd(const void *dy, const void *x, void *dx, int N, int H, int W, int C, void *stream);
+/* dx [N][Hh][Wh][C] = (x > 0) * sum of dy over the 4 nearest-upsampling children */
+int otf_unet_up2_bwd(const void *dy, const void *x, void *dx, int N, int Hh, int Wh, int C, void *stream);
+/* FP32 [npix][cin] -> BF16 [npix][16], channels >= cin zero */
+int otf_unet_pack_input(const float *x, int cin, long long npix, void *y, void *stream);
+/* out[p] = b + sum_c x[p][c] w[c], x [npix][32] BF16, FP32 out */
+int otf_unet_head(const void *x, const float *w, const float *b, long long npix, float *out, void *stream);
+/* dx = dout * w * (x > 0) (BF16); dw += sum_p dout x; db += sum_p dout */
+int otf_unet_head_bwd(const void *x, const float *w, const float *dout, long long npix, void *dx, float *dw,
+                      float *db, void *stream);
+/* loss += sum w (out - target)^2 * inv_norm; dout = 2 w (out - target) inv_norm (weight optional) */
+int otf_unet_mse(const float *out, const float *target, const float *weight, long long n, float inv_norm,
+                 float *dout, float *loss, void *stream);
+/* Adam with bias correction (step counts from 1) and L2 weight decay on FP32 parameters */
+int otf_unet_adam(float *p, const float *g, float *m, float *v, long long n, float lr, float b1, float b2,
+                  float eps, int step, float weight_decay, void *stream);
+/* BF16 copies of FP32 weights [9][cout][cin]: wf (same layout) and wb
+ * [8 - tap][cin][cout] (the input-gradient convolution), wb optional */
+int otf_unet_pack_weights(const float *w, int cout, int cin, void *wf, void *wb, void *stream);
 
 #ifdef __cplusplus
 }

@@ -45,6 +45,8 @@ def _declare(lib):
         "otf_batch_reverse": [c_void_p, c_void_p, c_int, c_void_p, c_float, c_int],
         "otf_batch_shot_grad": [c_void_p, c_int, c_void_p, c_int],
         "otf_batch_sync": [c_void_p],
+        "otf_batch_objective": [c_void_p, c_int, c_void_p, c_int],
+        "otf_batch_illumination": [c_void_p, c_int, c_void_p, c_int],
         "otf_misfit": [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p,
                        c_longlong, c_void_p],
     }.items():
@@ -64,11 +66,16 @@ def _is_torch(a):
 
 
 def _ptr(a):
-    """(pointer, on_device) of a numpy array or torch CUDA tensor."""
+    """(pointer, on_device) of a numpy array or torch CUDA tensor. A CUDA
+    tensor's pending work on torch's current stream is waited for first: the
+    library reads and writes it on the batch's own stream."""
     if a is None:
         return None, 0
     if _is_torch(a):
         assert a.is_contiguous()
+        if a.is_cuda:
+            import torch
+            torch.cuda.current_stream(a.device).synchronize()
         return ctypes.c_void_p(a.data_ptr()), int(a.is_cuda)
     return ctypes.c_void_p(a.ctypes.data), 0
 
@@ -154,6 +161,8 @@ class ShotBatch:
             cquad = cquad.float().contiguous()
         p, dev = _ptr(cquad)
         self._ok(self._lib.otf_batch_set_model(self._h, p, dev))
+        if dev:
+            self.sync()  # the library reads the tensor on its own stream
         self._keep_model = cquad
 
     def set_observed(self, obs):
@@ -161,6 +170,8 @@ class ShotBatch:
             obs = _f32(obs)
         p, dev = _ptr(obs)
         self._ok(self._lib.otf_batch_set_observed(self._h, p, dev))
+        if dev:
+            self.sync()
         self._keep_obs = obs
 
     def set_precision(self, precision):
@@ -187,8 +198,7 @@ class ShotBatch:
         p, dev = _ptr(out)
         f = self._lib.otf_batch_forward_ring if ring else self._lib.otf_batch_forward
         self._ok(f(self._h, p, dev))
-        if not dev:
-            self.sync()
+        self.sync()
         return out
 
     def gradient(self, misfit="wasserstein", grad=None, misfit_out=None):
@@ -201,10 +211,32 @@ class ShotBatch:
             misfit_out = np.zeros(1, np.float64) if not dev else None
         mp, _ = _ptr(misfit_out)
         self._ok(self._lib.otf_batch_gradient(self._h, kind, gp, mp, dev))
+        self.sync()
         if not dev:
-            self.sync()
             return grad, float(misfit_out[0])
         return grad, misfit_out
+
+    def objective(self, misfit="wasserstein", out=None):
+        """Total misfit of a forward of every shot (no reverse phase): a
+        line-search evaluation, one graph replay. ``out``: optional float64
+        device tensor of one element."""
+        kind = MISFITS[misfit] if isinstance(misfit, str) else int(misfit)
+        host = out is None
+        if host:
+            out = np.zeros(1, np.float64)
+        p, dev = _ptr(out)
+        self._ok(self._lib.otf_batch_objective(self._h, kind, p, dev))
+        self.sync()
+        return float(out[0]) if host else out
+
+    def illumination(self, every=8, out=None):
+        """Sum over shots and every ``every``-th forward step of P^2, [Z, X]."""
+        if out is None:
+            out = np.zeros((self.Z, self.X), np.float32)
+        p, dev = _ptr(out)
+        self._ok(self._lib.otf_batch_illumination(self._h, int(every), p, dev))
+        self.sync()
+        return out
 
     def misfit(self, misfit="wasserstein"):
         kind = MISFITS[misfit] if isinstance(misfit, str) else int(misfit)
@@ -226,8 +258,7 @@ class ShotBatch:
             grad = np.zeros((self.Z, self.X), np.float32)
         gp, gdev = _ptr(grad)
         self._ok(self._lib.otf_batch_reverse(self._h, ap, adev, gp, float(scale), gdev))
-        if not gdev:
-            self.sync()
+        self.sync()
         return grad
 
     def shot_gradient(self, shot):
@@ -302,10 +333,9 @@ class MultiBatch:
         """[(grad [Z, X], misfit)] of every instance from one graph launch."""
         kind = MISFITS[misfit] if isinstance(misfit, str) else int(misfit)
         L = self._lib
-        for rc in (L.otf_multi_gradient(self._h, kind), L.otf_multi_sync(self._h)):
-            if rc != 0:
-                _lib.check(L)
-                raise _lib.OtfwiError("multi-instance gradient failed")
+        if L.otf_multi_gradient(self._h, kind) != 0 or L.otf_multi_sync(self._h) != 0:
+            _lib.check(L)
+            raise _lib.OtfwiError("multi-instance gradient failed")
         out = []
         for b in self.batches:
             g = np.zeros((b.Z, b.X), np.float32)

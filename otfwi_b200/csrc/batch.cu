@@ -181,6 +181,27 @@ int otf_batch_backward_exact(otf_batch *b, const float *g, int g_on_device, floa
 
 int otf_batch_sync(otf_batch *b) { return b->eng.sync(); }
 
+int otf_batch_objective(otf_batch *b, int misfit_kind, double *misfit, int on_device)
+{
+    if (b->eng.objective(misfit_kind))
+        return -1;
+    if (misfit)
+        OTF_CUDA(cudaMemcpyAsync(misfit, b->eng.misfit_total_dev(), sizeof(double), kind_out(on_device),
+                                 b->eng.stream()));
+    return 0;
+}
+
+int otf_batch_illumination(otf_batch *b, int every, float *illum, int on_device)
+{
+    if (b->eng.illumination(every))
+        return -1;
+    const otf::EngineConfig &c = b->eng.config();
+    if (illum)
+        OTF_CUDA(cudaMemcpyAsync(illum, b->eng.illum_dev(), sizeof(float) * (size_t)c.X * c.Z,
+                                 kind_out(on_device), b->eng.stream()));
+    return 0;
+}
+
 int otf_batch_last_gradient(otf_batch *b, float *grad, double *misfit, int on_device)
 {
     const otf::EngineConfig &c = b->eng.config();

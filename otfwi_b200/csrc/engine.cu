@@ -285,6 +285,15 @@ void Engine::drop_graphs()
             cudaGraphExecDestroy(g);
         g = nullptr;
     }
+    for (auto &g : g_obj_) {
+        if (g)
+            cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    if (g_illum_)
+        cudaGraphExecDestroy(g_illum_);
+    g_illum_ = nullptr;
+    illum_every_ = 0;
     graph_shots_ = -1;
 }
 
@@ -294,7 +303,7 @@ void Engine::free_all()
     if (qr_ == qf_)
         qr_ = nullptr;  // aliased when dt == dx == 1: freed once, as qf_
     float **fl[] = {&qf_, &qr_, &dampx_, &dampz_, &dampx2_, &dampz2_, &grad_, &rec_, &ring_,
-                    &src_, &tab_src_, &adj_, &tab_adj_, &obs_};
+                    &src_, &tab_src_, &adj_, &tab_adj_, &obs_, &gsum_, &illum_};
     for (float **p : fl) {
         if (*p)
             cudaFree(*p);
@@ -303,6 +312,9 @@ void Engine::free_all()
     if (mis_)
         cudaFree(mis_);
     mis_ = nullptr;
+    if (tot_)
+        cudaFree(tot_);
+    tot_ = nullptr;
     if (mscratch_)
         cudaFree(mscratch_);
     mscratch_ = nullptr;
@@ -1101,6 +1113,93 @@ int Engine::gradient(int kind)
     if (!g_grad_[kind] && capture(&g_grad_[kind], [&] { return emit_gradient(kind); }))
         return -1;
     OTF_CUDA(cudaGraphLaunch(g_grad_[kind], st_));
+    return 0;
+}
+
+// Forward of every shot and the device misfit only (no ring, no reverse
+// phase): the objective evaluations of a line search.
+int Engine::objective(int kind)
+{
+    if (prepare_gradient(kind))
+        return -1;
+    if (!g_obj_[kind] &&
+        capture(&g_obj_[kind], [&] { return (emit_forward(false) || misfit(kind, tot_)) ? -1 : 0; }))
+        return -1;
+    OTF_CUDA(cudaGraphLaunch(g_obj_[kind], st_));
+    return 0;
+}
+
+// illum[z][x] += sum over shots of P(x, z)^2 at the current output slot.
+// P is the total pressure: the split field P of the strip-split kernels, or
+// Px + Pz of the others.
+__global__ void k_illum(const float *__restrict__ px, const float *__restrict__ pz,
+                        float *__restrict__ illum, Layout L, int n_shots, int64_t stride)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)L.X * L.Z)
+        return;
+    const int z = (int)(i / L.X), x = (int)(i - (int64_t)z * L.X);
+    const int64_t o = L.at(x, z);
+    float acc = 0.f;
+    for (int s = 0; s < n_shots; s++) {
+        const float v = pz ? px[o + stride * s] + pz[o + stride * s] : px[o + stride * s];
+        acc = fmaf(v, v, acc);
+    }
+    illum[i] += acc;
+}
+
+// Source illumination: sum over shots and over every `every`-th forward step
+// of P^2, into illum_dev() ([Z*X], overwritten). A diagonal pseudo-Hessian
+// used to normalise gradients; one forward per call.
+int Engine::illumination(int every)
+{
+    if (prepare())
+        return -1;
+    OTF_CHECK(every >= 1, 1, "illumination interval must be >= 1");
+    if (!illum_)
+        OTF_CUDA(cudaMalloc(&illum_, sizeof(float) * (size_t)cfg_.X * cfg_.Z));
+    float *illum_dev = illum_;
+    if (g_illum_ && illum_every_ != every) {
+        cudaGraphExecDestroy(g_illum_);
+        g_illum_ = nullptr;
+    }
+    const bool split = variant_in_use() == 2;
+    const int64_t n = (int64_t)cfg_.X * cfg_.Z;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    auto emit = [&]() -> int {
+        OTF_CUDA(cudaMemsetAsync(illum_dev, 0, sizeof(float) * (size_t)n, st_));
+        StepParams p = base_params();
+        p.q0 = qf_;
+        p.q1 = qf_;
+        p.inj_ptr = inj_src_ptr_;
+        p.inj_x = inj_src_x_;
+        p.inj_z = inj_src_z_;
+        p.inj_row = inj_src_row_;
+        p.inj_tab = tab_src_;
+        const dim3 grid = step_grid(cfg_, n_shots_);
+        const size_t fbytes = sizeof(float) * (size_t)L_.slot * n_shots_;
+        for (int f = 0; f < 4; f++)
+            for (int s = 0; s < 2; s++)
+                OTF_CUDA(cudaMemsetAsync(fld_[0][f][s], 0, fbytes, st_));
+        for (int t = 1; t < cfg_.T; t++) {
+            const int i = (t - 1) & 1, o = t & 1;
+            p.t = t;
+            p.f0 = Fields{fld_[0][0][i], fld_[0][1][i], fld_[0][2][i], fld_[0][3][i],
+                          fld_[0][0][o], fld_[0][1][o], fld_[0][2][o], fld_[0][3][o]};
+            if (launch_forward_step(p, false, grid, i, i))
+                return -1;
+            if (t % every == 0) {
+                k_illum<<<nb, 256, 0, st_>>>(fld_[0][0][o], split ? nullptr : fld_[0][1][o], illum_dev, L_,
+                                             n_shots_, L_.slot);
+                OTF_CUDA(cudaGetLastError());
+            }
+        }
+        return 0;
+    };
+    if (!g_illum_ && capture(&g_illum_, emit))
+        return -1;
+    illum_every_ = every;
+    OTF_CUDA(cudaGraphLaunch(g_illum_, st_));
     return 0;
 }
 

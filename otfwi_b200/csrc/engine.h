@@ -69,6 +69,11 @@ class Engine {
     // the same work as an uninstantiated graph (caller owns it), for
     // composing several engines into one launch
     int gradient_graph(int kind, cudaGraph_t *out);
+    // forward + device misfit of every shot; total in misfit_total_dev()
+    int objective(int kind);
+    // sum over shots and every `every`-th step of P^2 into illum_dev() [Z*X]
+    int illumination(int every);
+    float *illum_dev() { return illum_; }
 
     // Differentiable path (engine_adjoint.cu): forward of every shot keeping
     // the full state every `every` steps (sqrt(T) checkpoints), then the
@@ -149,6 +154,10 @@ class Engine {
 
     cudaGraphExec_t g_fwd_ = nullptr, g_fwd_ring_ = nullptr, g_rev_ = nullptr;
     cudaGraphExec_t g_grad_[3] = {nullptr, nullptr, nullptr};  // per misfit kind
+    cudaGraphExec_t g_obj_[3] = {nullptr, nullptr, nullptr};   // forward + misfit
+    cudaGraphExec_t g_illum_ = nullptr;
+    int illum_every_ = 0;
+    float *illum_ = nullptr;  // [Z*X] illumination of the last illumination()
     float *gsum_ = nullptr;  // [Z*X] shot-mean gradient of the last gradient()
     double *tot_ = nullptr;  // misfit total of the last gradient()
     int graph_shots_ = -1;

@@ -80,7 +80,6 @@ __device__ __forceinline__ FF div(FF a, FF b)
     return add(q, ff(q3));
 }
 __device__ __forceinline__ bool lt(FF a, FF b) { return a.hi < b.hi || (a.hi == b.hi && a.lo < b.lo); }
-__device__ __forceinline__ bool ge(FF a, FF b) { return !lt(a, b); }
 
 __device__ __forceinline__ FF shfl_up(FF v, int d)
 {
