@@ -118,9 +118,11 @@ int otf_batch_set_model(otf_batch *b, const float *cquad, int on_device);       
 int otf_batch_set_observed(otf_batch *b, const float *obs, int on_device);      /* [n_shots*n_rec*T] */
 int otf_batch_set_precision(otf_batch *b, int precision);
 int otf_batch_set_tile(otf_batch *b, int tile);
-/* 0: one tile per CTA per step; 1 (default): persistent CTAs with TMA
- * double-buffered halo tiles (tile shapes 0, 1 and 4; others use 0).
- * Both give bit-identical results. */
+/* -1 (default): automatic, 2 with fast numerics and 1 otherwise; 0: one
+ * tile per CTA per step; 1: persistent CTAs with TMA double-buffered halo
+ * tiles (tile shapes 0, 1 and 4; others use 0); 2: persistent strip-split
+ * kernels, fast numerics only (tile shapes 0, 1 and 4). 0 and 1 give
+ * bit-identical results. */
 int otf_batch_set_kernel(otf_batch *b, int variant);
 /* Forward modelling of every shot; traces [n_shots][n_rec][T] (NULL: keep). */
 int otf_batch_forward(otf_batch *b, float *traces, int on_device);
@@ -128,8 +130,9 @@ int otf_batch_forward(otf_batch *b, float *traces, int on_device);
 int otf_batch_forward_ring(otf_batch *b, float *traces, int on_device);
 /* Full gradient: forward, device misfit (0 = L2, 1 = Wasserstein as
  * adjoint_functions.wasserstein, 2 = Wasserstein on softplus-normalised
- * traces), reverse phase; grad [Z*X] = mean over shots of the per-shot
- * gradients, *misfit = sum over every trace (both optional). */
+ * traces, 3 = adjoint_functions.wasserstein_quad), reverse phase; grad [Z*X]
+ * = mean over shots of the per-shot gradients, *misfit = sum over every
+ * trace (both optional). */
 int otf_batch_gradient(otf_batch *b, int misfit_kind, float *grad, double *misfit, int on_device);
 /* Device misfit of the last forward traces against the observed traces:
  * per-trace misfits [n_shots*n_rec] (optional) and the adjoint sources. */

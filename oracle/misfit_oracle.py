@@ -162,3 +162,70 @@ def wasserstein_softplus(sim, obs):
         out[s] = adj
         W2 += w2
     return W2, out
+
+
+def wasserstein_quad_trace(sim_s, obs_s, t, dt):
+    """One trace of adjoint_functions.py:70-108 (wasserstein_quad): densities
+    sim^2 + c and obs^2 + c with c = 0.05 max(obs^2), each keeping its input
+    dtype as in the reference (the callback passes float64 sim and float32
+    obs), rectangle-normalised, rectangle-rule CDFs (cumsum * dt); returns
+    (W2 term, adjoint row)."""
+    g = np.asarray(obs_s) ** 2
+    f = np.asarray(sim_s) ** 2
+    c = np.max(g) * 0.05
+    g += c
+    f += c
+    g /= np.sum(g * dt)
+    f /= np.sum(f * dt)
+    G = np.cumsum(g * dt)
+    F = np.cumsum(f * dt)
+    F_i = Interp1dLinear(t, F)
+    F_1 = Interp1dLinear(F, t)
+    G_1 = Interp1dLinear(G, t)
+    dist = Interp1dLinear(t, 2 * np.cumsum(t - G_1(F_i(t))) * dt)
+    adj = dist(t) - dist(1)
+    w2 = sum(np.abs(F_1(t) - G_1(t)) ** 2)
+    return w2, adj
+
+
+def wasserstein_quad(sim, obs):
+    """adjoint_functions.py:70-108: Wasserstein misfit of squared traces."""
+    sim = np.asarray(sim)
+    obs = np.asarray(obs)
+    n_sens, T = sim.shape
+    t = np.linspace(0, 1, T)
+    dt = t[1] - t[0]
+    W2 = 0
+    s_W2 = np.zeros((n_sens, T))
+    for s in range(n_sens):
+        w2, adj = wasserstein_quad_trace(sim[s], obs[s], t, dt)
+        s_W2[s, :] = adj
+        W2 += w2
+    return W2, s_W2
+
+
+def analytic_signal(x):
+    """scipy.signal.hilbert(x) along the last axis: FFT, one-sided spectrum
+    weights h (h[0] = 1, 2 on positive frequencies, h[N/2] = 1 for even N,
+    0 on negative frequencies), inverse FFT."""
+    x = np.asarray(x, dtype=np.float64)
+    N = x.shape[-1]
+    h = np.zeros(N)
+    if N % 2 == 0:
+        h[0] = h[N // 2] = 1
+        h[1:N // 2] = 2
+    else:
+        h[0] = 1
+        h[1:(N + 1) // 2] = 2
+    return np.fft.ifft(np.fft.fft(x, axis=-1) * h, axis=-1)
+
+
+def quad_envelope(sim, obs):
+    """adjoint_functions.py:14-22: misfit sum((|H sim|^2 - |H obs|^2)^2) and
+    adjoint sim * e - Im(H(e * Im(H sim))), e = |H sim|^2 - |H obs|^2, H the
+    analytic signal."""
+    hs = analytic_signal(sim)
+    ho = analytic_signal(obs)
+    e = np.abs(hs) ** 2 - np.abs(ho) ** 2
+    adj = np.asarray(sim, np.float64) * e - np.imag(analytic_signal(e * np.imag(hs)))
+    return np.sum(e ** 2), adj

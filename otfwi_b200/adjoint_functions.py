@@ -9,6 +9,7 @@ init_regression`` as the adjoint callback:
   wasserstein           adjoint_functions.py:25-67
   wasserstein_softplus  Wasserstein on softplus-normalised traces (no
                         reference counterpart; definition in misfit.cu)
+  wasserstein_quad      adjoint_functions.py:70-108
 
 The arithmetic runs in the library's misfit kernels (otf_misfit); device
 memory comes from PyTorch. No CPU fallback: without a GPU these raise.
@@ -56,3 +57,7 @@ def wasserstein(sim, obs):
 
 def wasserstein_softplus(sim, obs):
     return _device_misfit(MISFITS["wasserstein_softplus"], sim, obs)
+
+
+def wasserstein_quad(sim, obs):
+    return _device_misfit(MISFITS["wasserstein_quad"], sim, obs)

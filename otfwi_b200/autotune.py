@@ -84,8 +84,10 @@ def time_config(sc, kernel, tile, precision, T_proxy, misfit, reps=2):
         b.close()
 
 
-def autotune(sc, precision=1, misfit="wasserstein_softplus", T_proxy=300, use_cache=True, verbose=False):
-    """Best (kernel, tile) for a scenario; returns (kernel, tile, table)."""
+def autotune(sc, precision=1, misfit="wasserstein_softplus", T_proxy=300, use_cache=True, verbose=False,
+             cands=None):
+    """Best (kernel, tile) for a scenario; returns (kernel, tile, table).
+    ``cands``: [(kernel, tile)] to try instead of every compiled candidate."""
     import torch
     gpu = torch.cuda.get_device_name()
     key = _key(sc.X, sc.Z, sc.n_src, sc.n_rec, precision, gpu)
@@ -94,7 +96,7 @@ def autotune(sc, precision=1, misfit="wasserstein_softplus", T_proxy=300, use_ca
         e = cache[key]
         return e["kernel"], e["tile"], e.get("table", {})
     table = {}
-    for kernel, tile in candidates(precision):
+    for kernel, tile in (cands if cands is not None else candidates(precision)):
         t0 = time.perf_counter()
         try:
             ms = time_config(sc, kernel, tile, precision, T_proxy, misfit)

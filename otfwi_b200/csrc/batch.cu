@@ -223,7 +223,7 @@ int otf_batch_last_gradient(otf_batch *b, float *grad, double *misfit, int on_de
 struct otf_multi {
     std::vector<otf_batch *> b;
     cudaStream_t st = nullptr;
-    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+    cudaGraphExec_t exec[otf::kNumMisfits] = {};
     ~otf_multi()
     {
         for (auto &e : exec)
@@ -256,7 +256,7 @@ void otf_multi_destroy(otf_multi *m) { delete m; }
 
 int otf_multi_gradient(otf_multi *m, int misfit_kind)
 {
-    OTF_CHECK(misfit_kind >= 0 && misfit_kind < 3, 1, "unknown misfit kind");
+    OTF_CHECK(misfit_kind >= 0 && misfit_kind < otf::kNumMisfits, 1, "unknown misfit kind");
     if (!m->exec[misfit_kind]) {
         cudaGraph_t parent = nullptr;
         OTF_CUDA(cudaGraphCreate(&parent, 0));

@@ -1082,7 +1082,7 @@ int Engine::prepare_gradient(int kind)
 {
     if (prepare())
         return -1;
-    OTF_CHECK(kind >= 0 && kind < 3, 1, "unknown misfit kind");
+    OTF_CHECK(kind >= 0 && kind < kNumMisfits, 1, "unknown misfit kind");
     if (!gsum_) {
         OTF_CUDA(cudaMalloc(&gsum_, sizeof(float) * (size_t)cfg_.X * cfg_.Z));
         OTF_CUDA(cudaMalloc(&tot_, sizeof(double)));

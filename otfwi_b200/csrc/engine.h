@@ -8,6 +8,7 @@
 #include "pml_step.cuh"
 #include "pml_step_tma.cuh"
 #include "pml_step_split.cuh"
+#include "misfit.h"
 
 namespace otf {
 
@@ -153,8 +154,8 @@ class Engine {
     int *inj_adj_ptr_ = nullptr, *inj_adj_x_ = nullptr, *inj_adj_z_ = nullptr, *inj_adj_row_ = nullptr;
 
     cudaGraphExec_t g_fwd_ = nullptr, g_fwd_ring_ = nullptr, g_rev_ = nullptr;
-    cudaGraphExec_t g_grad_[3] = {nullptr, nullptr, nullptr};  // per misfit kind
-    cudaGraphExec_t g_obj_[3] = {nullptr, nullptr, nullptr};   // forward + misfit
+    cudaGraphExec_t g_grad_[kNumMisfits] = {};  // per misfit kind
+    cudaGraphExec_t g_obj_[kNumMisfits] = {};   // forward + misfit
     cudaGraphExec_t g_illum_ = nullptr;
     int illum_every_ = 0;
     float *illum_ = nullptr;  // [Z*X] illumination of the last illumination()

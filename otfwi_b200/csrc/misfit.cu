@@ -265,6 +265,8 @@ __global__ void __launch_bounds__(MT) k_wasserstein(const float *__restrict__ si
         af = block_minmax(af, true, redf);
         c = fmax(-1.1 * (double)mn, 0.1 * (double)mx);  // adjoint_functions.py:38-39
         s = am > 0.f ? 0.1 * (double)am : 1.0;
+        if (KIND == 3)  // c = 0.05 max(obs^2) in FP32 (adjoint_functions.py:79)
+            c = (double)__fmul_rn(__fmul_rn(am, am), 0.05f);
         // The normalisation p = f / sum(f dt) is scale-free, so the shifted
         // traces are brought to unit magnitude by an exact power of two:
         // float-float keeps FP64-class precision only for normal magnitudes.
@@ -272,12 +274,21 @@ __global__ void __launch_bounds__(MT) k_wasserstein(const float *__restrict__ si
         if (m > 0.0 && m < 1e30)
             scale = ldexpf(1.f, -ilogb(m));
     }
-    // densities up to a constant factor (scale for kind 1, 1/s for kind 2)
+    // densities up to a constant factor (scale for kind 1, 1/s for kind 2,
+    // scale^2 for kind 3, whose observed density is the reference's FP32
+    // obs^2 + c, adjoint_functions.py:76-82)
     const double cs = c * (double)scale;
+    const float sc2 = scale * scale, c32 = (float)c;
     auto pf = [&](int i) -> FF {
+        if (KIND == 3) {
+            const FF x = ff(__fmul_rn(f[i], scale));
+            return add(mul(x, x), ff(__fmul_rn(c32, sc2)));
+        }
         return KIND == 1 ? add(ff(__fmul_rn(f[i], scale)), ffd(cs)) : ffd(softplus_unit((double)f[i] / s));
     };
     auto pg = [&](int i) -> FF {
+        if (KIND == 3)
+            return ff(__fmul_rn(__fadd_rn(__fmul_rn(g[i], g[i]), c32), sc2));
         return KIND == 1 ? add(ff(__fmul_rn(g[i], scale)), ffd(cs)) : ffd(softplus_unit((double)g[i] / s));
     };
     // normalisation: divide by sum(p * dt) (adjoint_functions.py:43-44)
@@ -289,16 +300,25 @@ __global__ void __launch_bounds__(MT) k_wasserstein(const float *__restrict__ si
     const FF dtf = ffd(step);
     const FF Zf = mul(block_sum(sf, red), dtf);
     const FF Zg = mul(block_sum(sg, red), dtf);
-    // trapezoid CDFs with x = t (cumulative_trapezoid(., t, initial=0))
-    auto dti = [&](int i) { return ffd(tval(i, T, step) - tval(i - 1, T, step)); };
-    block_scan(Gs, T, [&](int i) -> FF {
-        if (i == 0) return FF{0.f, 0.f};
-        return mulf(mul(dti(i), add(div(pg(i), Zg), div(pg(i - 1), Zg))), 0.5f);
-    }, red);
-    block_scan(Fs, T, [&](int i) -> FF {
-        if (i == 0) return FF{0.f, 0.f};
-        return mulf(mul(dti(i), add(div(pf(i), Zf), div(pf(i - 1), Zf))), 0.5f);
-    }, red);
+    if (KIND == 3) {
+        // rectangle CDFs cumsum(p dt); the observed density is normalised in
+        // place in FP32 by the reference (adjoint_functions.py:82-86)
+        block_scan(Gs, T, [&](int i) -> FF {
+            return mul(ff(__double2float_rn(ff2d(div(pg(i), Zg)))), dtf);
+        }, red);
+        block_scan(Fs, T, [&](int i) -> FF { return mul(div(pf(i), Zf), dtf); }, red);
+    } else {
+        // trapezoid CDFs with x = t (cumulative_trapezoid(., t, initial=0))
+        auto dti = [&](int i) { return ffd(tval(i, T, step) - tval(i - 1, T, step)); };
+        block_scan(Gs, T, [&](int i) -> FF {
+            if (i == 0) return FF{0.f, 0.f};
+            return mulf(mul(dti(i), add(div(pg(i), Zg), div(pg(i - 1), Zg))), 0.5f);
+        }, red);
+        block_scan(Fs, T, [&](int i) -> FF {
+            if (i == 0) return FF{0.f, 0.f};
+            return mulf(mul(dti(i), add(div(pf(i), Zf), div(pf(i - 1), Zf))), 0.5f);
+        }, red);
+    }
     // F may be non-monotone (shifted simulated trace below zero): interp1d
     // then interpolates over the stably sorted (F, t) pairs
     if (threadIdx.x == 0)
@@ -336,13 +356,15 @@ __global__ void __launch_bounds__(MT) k_wasserstein(const float *__restrict__ si
     w2 = block_sum(w2, red);
     __syncthreads();
     // potential: 2 * cumulative_trapezoid(v, initial=0) with unit spacing
+    // (kind 3: 2 * cumsum(v) * dt, adjoint_functions.py:97)
     block_scan(Fs, T, [&](int i) -> FF {
+        if (KIND == 3) return mul(mulf(Ws[i], 2.f), dtf);
         if (i == 0) return FF{0.f, 0.f};
         return add(Ws[i], Ws[i - 1]);  // 2 * (v_i + v_{i-1}) / 2
     }, red);
     const FF last = Fs[T - 1];
     float *a = adj + (int64_t)tr * T;
-    if (KIND == 1) {
+    if (KIND == 1 || KIND == 3) {
         for (int i = threadIdx.x; i < T; i += MT)
             a[i] = __double2float_rn(ff2d(sub(Fs[i], last)));
     } else {
@@ -421,6 +443,9 @@ int launch_misfit(int kind, const float *sim, const float *obs, float *adj, doub
         break;
     case kMisfitWassersteinSoftplus:
         k_wasserstein<2><<<n_traces, MT, 0, st>>>(sim, obs, adj, misfit, (char *)scratch, T, per);
+        break;
+    case kMisfitWassersteinQuad:
+        k_wasserstein<3><<<n_traces, MT, 0, st>>>(sim, obs, adj, misfit, (char *)scratch, T, per);
         break;
     default:
         OTF_CHECK(false, 1, "misfit: unknown kind");

@@ -5,7 +5,13 @@
 
 namespace otf {
 
-enum MisfitKind : int { kMisfitL2 = 0, kMisfitWasserstein = 1, kMisfitWassersteinSoftplus = 2 };
+enum MisfitKind : int {
+    kMisfitL2 = 0,
+    kMisfitWasserstein = 1,
+    kMisfitWassersteinSoftplus = 2,
+    kMisfitWassersteinQuad = 3
+};
+constexpr int kNumMisfits = 4;
 
 // Bytes of global scratch one trace needs (0 for L2).
 int64_t misfit_scratch_per_trace(int kind, int T);

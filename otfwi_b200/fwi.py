@@ -122,21 +122,20 @@ class Problem:
         return sb.objective(self.misfit)
 
     def rms(self, c):
-        """RMS velocity error in m/s over the whole grid."""
-        d = (c - self.c_true) * float(self.sc.c_max / 0.4)
-        return float(self.torch.sqrt(self.torch.mean(d * d)).item())
+        """RMS velocity error in m/s over the inverted region (gmask > 0)."""
+        d = (c - self.c_true) * float(self.sc.c_max / 0.4) * self.gmask
+        return float(self.torch.sqrt(self.torch.sum(d * d) / self.gmask.sum()).item())
 
     def clip(self, c):
         return self.torch.clamp(c, self.vmin, self.vmax)
 
 
-def default_gmask(sc, margin=6):
-    """1 inside the PML-free region below the array, 0 elsewhere (the
-    reference's gmask zeroes the gradient near sources and boundaries)."""
+def default_gmask(sc):
+    """1 on the central rectangle of half the grid's height and width, 0
+    elsewhere, as the reference's setups draw it
+    (setups/setup1_OCNDT.py:82-84)."""
     m = np.zeros((sc.Z, sc.X), np.float32)
-    zs = np.where(sc.rec_mask)[0]
-    z0 = (int(zs.max()) if len(zs) else sc.PML) + margin
-    m[z0:sc.Z - sc.PML - margin, sc.PML + margin:sc.X - sc.PML - margin] = 1.0
+    m[sc.Z // 4:sc.Z - sc.Z // 4, sc.X // 4:sc.X - sc.X // 4] = 1.0
     return m
 
 
@@ -191,12 +190,14 @@ def line_search(prob, b, c, d, J0, alpha0, max_evals=6):
     return best_a, best_J, evals
 
 
-def descent(prob, c0, proposer=None, alpha0=None, on_iter=None):
+def descent(prob, c0, proposer=None, alpha0=None, on_step=None, on_iter=None):
     """Gradient descent with line search over the bands (the model stays on
     the GPU). With ``proposer(prob, band, c, g, J)`` -> update (device) the
     proposal is tried first and accepted only if the misfit decreases; the
-    plain step is the fallback. Returns (c, History); timing is wall clock
-    with the device synchronised at every accepted iterate."""
+    plain step is the fallback. ``on_step(b, it, c, g, J)`` is called with
+    every gradient, ``on_iter(b, it, c_new, g, J_old, J_new)`` after every
+    accepted step. Returns (c, History); timing is wall clock with the device
+    synchronised at every accepted iterate."""
     torch = prob.torch
     c = prob.clip(torch.as_tensor(np.asarray(c0, np.float32)).cuda().clone())
     h = History()
@@ -217,6 +218,8 @@ def descent(prob, c0, proposer=None, alpha0=None, on_iter=None):
         for it in range(band.iters):
             g, J0 = prob.gradient(b, c)
             evals_total += 92.0 / 28.0  # a gradient costs 92/28 forward modellings
+            if on_step is not None:
+                on_step(b, it, c, g, J0)
             used_learned = False
             if proposer is not None:
                 dc = proposer(prob, b, c, g, J0)

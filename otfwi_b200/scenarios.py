@@ -70,6 +70,41 @@ def circle_defects(X, Z, c_bg, c_def, n_def, rmin, rmax, lo, hi, rng):
     return c
 
 
+def gaussian_smooth(a, sigma):
+    """Separable Gaussian filter (truncated at 4 sigma, reflected edges)."""
+    r = int(4 * sigma + 0.5)
+    k = np.exp(-0.5 * (np.arange(-r, r + 1) / sigma) ** 2)
+    k /= k.sum()
+    out = np.asarray(a, np.float64)
+    for ax in (0, 1):
+        pad = [(0, 0), (0, 0)]
+        pad[ax] = (r, r)
+        p = np.pad(out, pad, mode="reflect")
+        out = sum(k[i] * np.take(p, np.arange(i, i + out.shape[ax]), axis=ax) for i in range(2 * r + 1))
+    return out
+
+
+def heterogeneous_defects(X, Z, rng, n_def=8, c_bg=5900.0, v_lo=4000.0, v_hi=6300.0, amin=4, amax=14,
+                          lo=None, hi=None, hetero=0.03, sigma=4.0):
+    """Velocity model in m/s: background c_bg with Gaussian-smoothed random
+    heterogeneity (sigma cells, +-hetero relative, peak-normalised) and n_def
+    elliptical defects (semi-axes amin..amax cells, random orientation,
+    velocities uniform in [v_lo, v_hi]) with centres uniform in [lo, hi]^2."""
+    lo = 0.25 * min(X, Z) if lo is None else lo
+    hi = 0.75 * min(X, Z) if hi is None else hi
+    h = gaussian_smooth(rng.standard_normal((Z, X)), sigma)
+    c = c_bg * (1.0 + hetero * h / np.abs(h).max())
+    zz, xx = np.mgrid[0:Z, 0:X]
+    for _ in range(n_def):
+        a, b = rng.uniform(amin, amax, size=2)
+        th = rng.uniform(0, np.pi)
+        cx, cz = rng.uniform(lo, hi, size=2)
+        u = (xx - cx) * np.cos(th) + (zz - cz) * np.sin(th)
+        v = -(xx - cx) * np.sin(th) + (zz - cz) * np.cos(th)
+        c[(u / a) ** 2 + (v / b) ** 2 <= 1.0] = rng.uniform(v_lo, v_hi)
+    return c
+
+
 def _array_masks(X, Z, xs, z, src_idx=None):
     rec = np.zeros((Z, X), dtype=bool)
     rec[z, xs] = True

@@ -309,3 +309,49 @@ class UNet:
         self.backward(self._buffers(N, H, W)["dout"])
         self.adam(lr)
         return loss
+
+
+def _bench(argv=None):
+    """Time forward and training steps: python -m otfwi_b200.unet --n 16 --hw 256."""
+    import argparse
+    import json
+
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=16)
+    ap.add_argument("--hw", type=int, default=256)
+    ap.add_argument("--iters", type=int, default=10)
+    a = ap.parse_args(argv)
+    net = UNet(base=32)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    x = torch.randn(a.n, a.hw, a.hw, 3, device="cuda", generator=g)
+    t = 0.01 * torch.randn(a.n, a.hw, a.hw, device="cuda", generator=g)
+    for _ in range(3):
+        net.train_step(x, t)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.iters):
+        net.forward(x)
+    e1.record()
+    torch.cuda.synchronize()
+    f_ms = e0.elapsed_time(e1) / a.iters
+    e0.record()
+    for _ in range(a.iters):
+        net.train_step(x, t)
+    e1.record()
+    torch.cuda.synchronize()
+    s_ms = e0.elapsed_time(e1) / a.iters
+    # 3x3 convolution FLOPs of one forward (2 per multiply-add); pooling,
+    # head and elementwise work excluded
+    flop = 0.0
+    for name, cin, cout in net.layers:
+        lvl = {"enc1": 0, "dec1": 0, "enc2": 1, "dec2": 1, "enc3": 2, "dec3": 2, "bota": 3, "botb": 3}[name[:4]]
+        flop += 2.0 * 9 * cin * cout * a.n * (a.hw >> lvl) ** 2
+    print(json.dumps({"n": a.n, "hw": a.hw, "forward_ms": f_ms, "forward_tflops": flop / f_ms / 1e9,
+                      "train_step_ms": s_ms, "train_tflops": 3 * flop / s_ms / 1e9}))
+
+
+if __name__ == "__main__":
+    _bench()

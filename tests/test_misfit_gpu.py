@@ -1,10 +1,10 @@
 """GPU misfit kernels against the reference's adjoint_functions outputs
 (tests/golden/misfit_*.npz) and the numpy oracle.
 
-Tolerances: L2 adjoint bit-identical, L2 misfit rel 1e-12; Wasserstein misfit
-rel 1e-5 and adjoint max|d| / max|ref| <= 1e-5 (compensated FP32 scans
-against the reference's FP64 numpy); softplus variant the same against the
-oracle's FP64 definition.
+Tolerances: L2 adjoint bit-identical, L2 misfit rel 1e-12; Wasserstein and
+wasserstein_quad misfit rel 1e-5 and adjoint max|d| / max|ref| <= 1e-5
+(compensated FP32 scans against the reference's FP64 numpy); softplus
+variant the same against the oracle's FP64 definition.
 """
 import glob
 import os
@@ -33,6 +33,9 @@ def test_device_misfits_match_reference(lib, path):
     m, adj = device_misfit(d["sim"], d["obs"], "wasserstein")
     assert abs(m.sum() - d["w2"]) <= 1e-5 * abs(d["w2"]), (m.sum(), d["w2"])
     assert _rel_max(adj, d["w2_adj"]) <= 1e-5
+    m, adj = device_misfit(d["sim"], d["obs"], "wasserstein_quad")
+    assert abs(m.sum() - d["w2q"]) <= 1e-5 * abs(d["w2q"]), (m.sum(), d["w2q"])
+    assert _rel_max(adj, d["w2q_adj"]) <= 1e-5
 
 
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "misfit_*.npz"))),
@@ -63,3 +66,7 @@ def test_wasserstein_long_traces_and_many(lib):
     ms, adjs = device_misfit(sim, obs, "wasserstein_softplus")
     assert abs(ms.sum() - w2s) <= 1e-5 * abs(w2s)
     assert _rel_max(adjs, refs) <= 1e-5
+    w2q, refq = mo.wasserstein_quad(sim.astype(np.float64), obs)
+    mq, adjq = device_misfit(sim, obs, "wasserstein_quad")
+    assert abs(mq.sum() - w2q) <= 1e-5 * abs(w2q)
+    assert _rel_max(adjq, refq) <= 1e-5

@@ -1,7 +1,8 @@
 """CPU tests of the oracle itself: pinned against the reference's own outputs.
 
 * misfit oracle vs tests/golden/misfit_*.npz (the reference's
-  adjoint_functions.wasserstein / L2, run unchanged): bit-exact;
+  adjoint_functions.wasserstein / L2 / wasserstein_quad, run unchanged):
+  bit-exact; quad_envelope within single-precision FFT rounding;
 * simulator oracle ("f32" mode) vs tests/golden/sim_*.npz (the reference's
   regression_PML_single.cu run on a GPU): traces and gradients;
 * "f32" vs "f64" mode agreement on the same inputs.
@@ -31,6 +32,20 @@ def test_misfit_oracle_matches_reference_bit_exact(path):
     l2, r = mo.L2(sim, d["obs"])
     assert l2 == d["l2"]
     assert np.array_equal(r, d["l2_adj"])
+    w2q, adjq = mo.wasserstein_quad(sim, d["obs"])
+    assert w2q == d["w2q"]
+    assert np.array_equal(adjq, d["w2q_adj"])
+
+
+@pytest.mark.parametrize("path", _misfit_cases(), ids=os.path.basename)
+def test_quad_envelope_oracle_vs_reference(path):
+    """The reference's analytic signal of the float32 observed trace goes
+    through scipy.fft in single precision; the oracle's is FP64, so the two
+    agree to single-precision FFT rounding, not bit for bit."""
+    d = np.load(path)
+    e, adj = mo.quad_envelope(d["sim"].astype(np.float64), d["obs"])
+    assert abs(e - d["env"]) <= 1e-6 * abs(d["env"])
+    assert np.max(np.abs(adj - d["env_adj"])) <= 1e-5 * np.max(np.abs(d["env_adj"]))
 
 
 def test_misfit_golden_covers_nonmonotone_cdf():
