@@ -190,11 +190,11 @@ def line_search(prob, b, c, d, J0, alpha0, max_evals=6):
     return best_a, best_J, evals
 
 
-def descent(prob, c0, proposer=None, alpha0=None, on_step=None, on_iter=None):
+def descent(prob, c0, proposer=None, alpha0=None, on_step=None, on_iter=None, proposal_scales=(1.0, 0.5)):
     """Gradient descent with line search over the bands (the model stays on
     the GPU). With ``proposer(prob, band, c, g, J)`` -> update (device) the
-    proposal is tried first and accepted only if the misfit decreases; the
-    plain step is the fallback. ``on_step(b, it, c, g, J)`` is called with
+    proposal is tried first, at each of ``proposal_scales`` in turn, and
+    accepted only if the misfit decreases; the plain step is the fallback. ``on_step(b, it, c, g, J)`` is called with
     every gradient, ``on_iter(b, it, c_new, g, J_old, J_new)`` after every
     accepted step. Returns (c, History); timing is wall clock with the device
     synchronised at every accepted iterate."""
@@ -223,11 +223,13 @@ def descent(prob, c0, proposer=None, alpha0=None, on_step=None, on_iter=None):
             used_learned = False
             if proposer is not None:
                 dc = proposer(prob, b, c, g, J0)
-                cand = prob.clip(c + dc)
-                Jc = prob.objective(b, cand)
-                evals_total += 1
-                if Jc < J0:
-                    c, J_new, used_learned = cand, Jc, True
+                for scale in proposal_scales:
+                    cand = prob.clip(c + scale * dc)
+                    Jc = prob.objective(b, cand)
+                    evals_total += 1
+                    if Jc < J0:
+                        c, J_new, used_learned = cand, Jc, True
+                        break
             if not used_learned:
                 d = -g * prob.gmask
                 gm = float(d.abs().max().item())

@@ -131,7 +131,7 @@ def generate(n_runs, seed0=1000, X=256, Z=256, T=1500, n_elem=32, pitch=6, n_src
     return torch.stack(xs), torch.stack(ys), weight, stats
 
 
-def train(net, X, Y, weight, steps=1500, batch=8, lr=1e-3, seed=0, log=None):
+def train(net, X, Y, weight, steps=4000, batch=16, lr=1e-3, seed=0, log=None):
     """Adam on the weighted MSE with cosine learning-rate decay and random
     horizontal flips; returns the loss history (host floats, every step)."""
     import torch
@@ -151,11 +151,11 @@ def train(net, X, Y, weight, steps=1500, batch=8, lr=1e-3, seed=0, log=None):
         wb = torch.where(flip[:, None, None], w.flip(2), w).contiguous()
         lr_s = lr * 0.5 * (1 + math.cos(math.pi * s / steps))
         net.forward(xb)
-        loss = net.loss_grad(yb, wb, inv_norm=inv)
+        loss = net.loss_grad(yb, wb, inv_norm=inv).clone()
         net.backward(net._buffers(*yb.shape)["dout"])
         net.adam(lr_s)
         losses.append(loss)
-        if log and (s % 200 == 0 or s == steps - 1):
+        if log and (s % 500 == 0 or s == steps - 1):
             log(f"step {s}: loss {float(loss.item()):.5f}")
     return [float(l.item()) for l in losses]
 
@@ -201,15 +201,16 @@ def evaluate(net, X=512, Z=512, T=4000, n_elem=64, pitch=6, n_src=64, iters=15, 
 def main(argv=None):
     ap = argparse.ArgumentParser(description="learned-preconditioned FWI: data, training, evaluation")
     ap.add_argument("--runs", type=int, default=256, help="plain FWI runs that generate training pairs")
-    ap.add_argument("--train-iters", type=int, default=8, help="plain iterations per band in data runs")
-    ap.add_argument("--steps", type=int, default=1500, help="training steps")
-    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--train-iters", type=int, default=10, help="plain iterations per band in data runs")
+    ap.add_argument("--steps", type=int, default=4000, help="training steps")
+    ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-grid", type=int, default=512)
     ap.add_argument("--eval-nt", type=int, default=4000)
     ap.add_argument("--eval-elements", type=int, default=64, help="elements per array (top and bottom)")
     ap.add_argument("--eval-shots", type=int, default=64)
     ap.add_argument("--eval-iters", type=int, default=15, help="iterations per band in the evaluation")
+    ap.add_argument("--eval-seeds", default="7", help="comma-separated model seeds of the evaluation")
     ap.add_argument("--weights", default=WEIGHTS, help="where to save / load the trained network")
     ap.add_argument("--skip-train", action="store_true", help="evaluate the saved network")
     ap.add_argument("--report", default=None, help="JSON report path")
@@ -237,10 +238,12 @@ def main(argv=None):
         del X, Y
     else:
         net = UNet.load(a.weights)
-    rep["eval"] = evaluate(net, X=a.eval_grid, Z=a.eval_grid, T=a.eval_nt, n_elem=a.eval_elements,
-                           n_src=a.eval_shots, iters=a.eval_iters, log=log)
-    ev = rep["eval"]
-    log(json.dumps({k: v for k, v in ev.items() if k != "history"}))
+    rep["eval"] = []
+    for seed in [int(x) for x in a.eval_seeds.split(",")]:
+        ev = evaluate(net, X=a.eval_grid, Z=a.eval_grid, T=a.eval_nt, n_elem=a.eval_elements, n_src=a.eval_shots,
+                      iters=a.eval_iters, seed=seed, log=log)
+        rep["eval"].append(ev)
+        log(json.dumps({k: v for k, v in ev.items() if k != "history"}))
     if a.report:
         with open(a.report, "w") as f:
             json.dump(rep, f)
