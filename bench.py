@@ -49,6 +49,7 @@ def parse():
                     help="tile shape index; -1 = chosen by the autotuner (otfwi_b200.autotune)")
     ap.add_argument("--kernel", type=int, default=int(os.environ.get("OTFWI_BENCH_KERNEL", "-1")),
                     help="-1 automatic, 0 per-tile, 1 persistent TMA, 2 persistent strip-split")
+    ap.add_argument("--stream-rows", type=int, default=64, help="segment rows of the z-streaming kernels")
     ap.add_argument("--X", type=int, default=512)
     ap.add_argument("--T", type=int, default=4000)
     ap.add_argument("--shots", type=int, default=64)
@@ -192,6 +193,7 @@ def run_ours(args):
         tuned = {"kernel": k, "tile": list(TILES[t]), "candidates_ms_T300": table}
     b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, prec_deriv=4,
                   precision=args.precision, tile=args.tile, kernel=args.kernel)
+    b.set_stream_rows(args.stream_rows)
     dev = torch.device("cuda", local)
     stream = torch.cuda.ExternalStream(b.stream(), device=dev)
     c_true = torch.tensor(sc.c_true, dtype=torch.float32, device=dev)
@@ -308,7 +310,8 @@ def run_ours(args):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded model, Ricker source; no external dataset)",
                 "config": dict(config_block(args, sc, f"shots-per-rank, gradient all-reduce, {world} rank(s)"),
-                               kernel_variant=args.kernel, tile=args.tile, autotune=tuned),
+                               kernel_variant=args.kernel, tile=args.tile, autotune=tuned,
+                               stream_rows=args.stream_rows if args.kernel == 3 else None),
                 "roofline": roof, "e2e": e2e,
                 # per step: T-1 forward + T-1 reverse step kernels, misfit,
                 # misfit sum, adjoint running integral, shot mean

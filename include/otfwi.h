@@ -121,9 +121,12 @@ int otf_batch_set_tile(otf_batch *b, int tile);
 /* -1 (default): automatic, 2 with fast numerics and 1 otherwise; 0: one
  * tile per CTA per step; 1: persistent CTAs with TMA double-buffered halo
  * tiles (tile shapes 0, 1 and 4; others use 0); 2: persistent strip-split
- * kernels, fast numerics only (tile shapes 0, 1 and 4). 0 and 1 give
- * bit-identical results. */
+ * kernels, fast numerics only (tile shapes 0, 1 and 4); 3: z-streaming
+ * strips of 120 columns, fast numerics, separable damping, X a multiple of 4
+ * (else 2). 0 and 1 give bit-identical results. */
 int otf_batch_set_kernel(otf_batch *b, int variant);
+/* Rows per segment of the z-streaming kernels (variant 3; default 64, >= 8). */
+int otf_batch_set_stream_rows(otf_batch *b, int rows);
 /* Forward modelling of every shot; traces [n_shots][n_rec][T] (NULL: keep). */
 int otf_batch_forward(otf_batch *b, float *traces, int on_device);
 /* Forward with boundary-ring recording (gradient phase 1). */

@@ -37,6 +37,7 @@ def _declare(lib):
         "otf_batch_set_precision": [c_void_p, c_int],
         "otf_batch_set_tile": [c_void_p, c_int],
         "otf_batch_set_kernel": [c_void_p, c_int],
+        "otf_batch_set_stream_rows": [c_void_p, c_int],
         "otf_batch_forward": [c_void_p, c_void_p, c_int],
         "otf_batch_forward_ring": [c_void_p, c_void_p, c_int],
         "otf_batch_gradient": [c_void_p, c_int, c_void_p, c_void_p, c_int],
@@ -182,8 +183,13 @@ class ShotBatch:
 
     def set_kernel(self, variant):
         """-1: automatic; 0: one tile per CTA per step; 1: persistent
-        TMA-pipelined CTAs; 2: persistent strip-split kernels (fast numerics)."""
+        TMA-pipelined CTAs; 2: persistent strip-split kernels (fast numerics);
+        3: z-streaming strips (fast numerics)."""
         self._ok(self._lib.otf_batch_set_kernel(self._h, variant))
+
+    def set_stream_rows(self, rows):
+        """Rows per segment of the z-streaming kernels (variant 3)."""
+        self._ok(self._lib.otf_batch_set_stream_rows(self._h, int(rows)))
 
     def sync(self):
         self._ok(self._lib.otf_batch_sync(self._h))

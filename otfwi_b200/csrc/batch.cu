@@ -66,6 +66,7 @@ int otf_batch_set_observed(otf_batch *b, const float *obs, int on_device)
 int otf_batch_set_precision(otf_batch *b, int precision) { return b->eng.set_precision(precision); }
 int otf_batch_set_tile(otf_batch *b, int tile) { return b->eng.set_tile(tile); }
 int otf_batch_set_kernel(otf_batch *b, int variant) { return b->eng.set_variant(variant); }
+int otf_batch_set_stream_rows(otf_batch *b, int rows) { return b->eng.set_stream_rows(rows); }
 
 int otf_batch_forward(otf_batch *b, float *traces, int on_device)
 {

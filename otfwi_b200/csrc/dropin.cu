@@ -96,6 +96,7 @@ void init_memory_sim(int x, int z, int t, float *cq, float *const_vec, float *d_
     cfg.precision = env_int("OTFWI_PRECISION", otf::kFaithful);
     cfg.tile = env_int("OTFWI_TILE", 0);
     if (s.eng.init(cfg, d_x_h, d_z_h) || s.eng.set_variant(env_int("OTFWI_KERNEL", -1)) ||
+        s.eng.set_stream_rows(env_int("OTFWI_STREAM_ROWS", 64)) ||
         s.eng.set_model(cq, false) ||
         s.eng.set_sources(ns, ps_x, ps_z, src) || s.eng.set_receivers(nm, pm_x, pm_z) ||
         s.eng.set_ring(0, nullptr, nullptr) || select_shot(s, -1))

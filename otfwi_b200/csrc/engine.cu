@@ -741,6 +741,71 @@ int Engine::build_tables()
             for (int n = 0; n < n_rec_; n++)
                 h.push_back(s * n_rec_ + n);
     }
+    // z-streaming kernels: point lists per (padded row, strip), key = (z +
+    // PAD) * n_strips + strip, column = x - (x0 - 4) within the strip's
+    // computed columns; ring ids of these kernels = position in the owned
+    // ring list (row-major order)
+    const int NS = (X + SO - 1) / SO, NR = L_.rows, NK = NR * NS;
+    struct SL {
+        std::vector<std::vector<std::pair<int, int>>> v;
+        size_t off = 0, n = 0;
+    };
+    SL s_src, s_rcv, s_sen, s_ringo, s_ringe;
+    for (SL *l : {&s_src, &s_rcv, &s_sen, &s_ringo, &s_ringe})
+        l->v.resize(NK);
+    auto key_of = [&](int z, int s) { return (z + PAD) * NS + s; };
+    auto each_strip = [&](int x, int z, int id, SL &l) {
+        for (int s = std::max(0, (x - 4) / SO - 1); s <= std::min(NS - 1, (x + 4) / SO + 1); s++)
+            if (x >= s * SO - 4 && x < s * SO + SO + 4)
+                l.v[key_of(z, s)].push_back({x - (s * SO - 4), id});
+    };
+    for (int k = 0; k < n_src_; k++)
+        each_strip(src_x_[k], src_z_[k], k, s_src);
+    for (int n = 0; n < n_rec_; n++) {
+        if (interior(rec_x_[n], rec_z_[n], X, Z))
+            each_strip(rec_x_[n], rec_z_[n], n, s_rcv);
+        s_sen.v[key_of(rec_z_[n], rec_x_[n] / SO)].push_back({rec_x_[n] % SO + 4, n});
+    }
+    for (int n = 0; n < n_ring_; n++)
+        s_ringo.v[key_of(ring_z_[n], ring_x_[n] / SO)].push_back({ring_x_[n] % SO + 4, n});
+    std::vector<int> ring_sid(n_ring_);
+    {
+        int pos = 0;
+        for (auto &v : s_ringo.v)
+            for (auto &e : v)
+                ring_sid[e.second] = pos++;
+    }
+    for (int n = 0; n < n_ring_; n++)
+        each_strip(ring_x_[n], ring_z_[n], ring_sid[n], s_ringe);
+    for (SL *l : {&s_src, &s_rcv, &s_sen, &s_ringo, &s_ringe}) {
+        std::vector<int> ptr(NK + 1, 0), col, id;
+        for (int k = 0; k < NK; k++) {
+            ptr[k + 1] = ptr[k] + (int)l->v[k].size();
+            for (auto &e : l->v[k]) {
+                col.push_back(e.first);
+                id.push_back(e.second);
+            }
+        }
+        l->off = h.size();
+        l->n = col.size();
+        h.insert(h.end(), ptr.begin(), ptr.end());
+        h.insert(h.end(), col.begin(), col.end());
+        h.push_back(0);
+        h.insert(h.end(), id.begin(), id.end());
+        h.push_back(0);
+    }
+    const size_t o_redge = h.size();
+    for (int rr = 0; rr < NR; rr++) {
+        const int z = rr - PAD;
+        h.push_back((!sep_ || z < 4 || z >= Z - 4 || hdampz_[rr] != 1.f) ? 1 : 0);
+    }
+    const size_t o_sedge = h.size();
+    for (int s = 0; s < NS; s++) {
+        bool edge = !sep_;
+        for (int x = s * SO - 4; !edge && x < s * SO + SO + 4; x++)
+            edge = x < 4 || x >= X - 4 || hdampx_[x + PAD] != 1.f;
+        h.push_back(edge ? 1 : 0);
+    }
     if (h.size() > tabs_cap_) {
         if (tabs_)
             cudaFree(tabs_);
@@ -782,6 +847,20 @@ int Engine::build_tables()
         rcve_id_ = rcve_cell_ + ne + 1;
     }
     tile_edge_ = d + o_edge;
+    auto lst = [&](const SL &l, const int *&ptr, const int *&col, const int *&id) {
+        ptr = d + l.off;
+        col = ptr + NK + 1;
+        id = col + l.n + 1;
+    };
+    const int *unused_id = nullptr;
+    lst(s_src, stb_.src_ptr, stb_.src_col, stb_.src_id);
+    lst(s_rcv, stb_.rcv_ptr, stb_.rcv_col, stb_.rcv_id);
+    lst(s_sen, stb_.sen_ptr, stb_.sen_col, stb_.sen_id);
+    lst(s_ringo, stb_.ring_ptr, stb_.ring_col, unused_id);
+    lst(s_ringe, stb_.ringe_ptr, stb_.ringe_col, stb_.ringe_id);
+    stb_.row_edge = d + o_redge;
+    stb_.strip_edge = d + o_sedge;
+    n_strips_ = NS;
     tables_dirty_ = false;
     drop_graphs();
     return 0;
@@ -845,14 +924,54 @@ static int resolve_variant(const KernelSet &k, int requested, int precision)
 
 int Engine::variant_in_use() const
 {
-    return resolve_variant(ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0], variant_, cfg_.precision);
+    const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
+    if (variant_ == 3 && cfg_.precision == kFast && sep_ && cfg_.X % 4 == 0)
+        return 3;
+    return resolve_variant(k, variant_ == 3 ? 2 : variant_, cfg_.precision);
+}
+
+// Persistent grid of a z-streaming kernel: resident CTAs per SM x SMs.
+template <class F>
+static int stream_grid(F f)
+{
+    int dev = 0, nsm = 0, nb = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, SC, 0) != cudaSuccess)
+        return 0;
+    return nb * nsm;
+}
+
+int Engine::launch_stream(const StepParams &p, int kind)
+{
+    static int grid[3] = {0, 0, 0};  // forward, forward with ring, reverse
+    StreamParams P;
+    P.p = p;
+    P.tb = stb_;
+    P.n_strips = n_strips_;
+    P.seg_h = seg_h_;
+    P.n_segs = (cfg_.Z + seg_h_ - 1) / seg_h_;
+    P.n_items = n_strips_ * P.n_segs * n_shots_;
+    P.err = derr_;
+    const void *fn = kind == 0 ? (const void *)k_forward_stream<false>
+                   : kind == 1 ? (const void *)k_forward_stream<true> : (const void *)k_reverse_stream<3>;
+    if (!grid[kind]) {
+        grid[kind] = kind == 0 ? stream_grid(k_forward_stream<false>)
+                   : kind == 1 ? stream_grid(k_forward_stream<true>) : stream_grid(k_reverse_stream<3>);
+        OTF_CHECK(grid[kind] > 0, 4, "z-streaming kernel does not fit on an SM");
+    }
+    void *args[] = {(void *)&P};
+    OTF_CUDA(cudaLaunchKernel(fn, dim3((unsigned)std::min(grid[kind], P.n_items)), dim3(SC), args, 0, st_));
+    return 0;
 }
 
 // One forward step launch. pin / ain: slots holding P(t-1) / A(t-1).
 int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, int pin, int ain)
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
-    const int v = resolve_variant(k, variant_, cfg_.precision);
+    const int v = variant_in_use();
+    if (v == 3)
+        return launch_stream(p, with_ring ? 1 : 0);
     if (v >= 1) {
         TmaParams P = *tmap_;
         P.p = p;
@@ -883,7 +1002,9 @@ int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, 
 int Engine::launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain, int in1)
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
-    const int v = resolve_variant(k, variant_, cfg_.precision);
+    const int v = variant_in_use();
+    if (v == 3)
+        return launch_stream(p, 2);
     if (v >= 1) {
         TmaParams P = *tmap_;
         P.p = p;
@@ -935,9 +1056,19 @@ int Engine::build_maps()
     return 0;
 }
 
+int Engine::set_stream_rows(int rows)
+{
+    OTF_CHECK(rows >= 8, 1, "stream segment rows must be >= 8");
+    if (rows != seg_h_) {
+        seg_h_ = rows;
+        drop_graphs();
+    }
+    return 0;
+}
+
 int Engine::set_variant(int variant)
 {
-    OTF_CHECK(variant >= -1 && variant <= 2, 1, "unknown kernel variant");
+    OTF_CHECK(variant >= -1 && variant <= 3, 1, "unknown kernel variant");
     if (variant != variant_) {
         variant_ = variant;
         drop_graphs();
@@ -1163,7 +1294,7 @@ int Engine::illumination(int every)
         cudaGraphExecDestroy(g_illum_);
         g_illum_ = nullptr;
     }
-    const bool split = variant_in_use() == 2;
+    const bool split = variant_in_use() >= 2;  // P total in the first field
     const int64_t n = (int64_t)cfg_.X * cfg_.Z;
     const unsigned nb = (unsigned)((n + 255) / 256);
     auto emit = [&]() -> int {

@@ -8,6 +8,7 @@
 #include "pml_step.cuh"
 #include "pml_step_tma.cuh"
 #include "pml_step_split.cuh"
+#include "pml_step_stream.cuh"
 #include "misfit.h"
 
 namespace otf {
@@ -97,8 +98,12 @@ class Engine {
     int set_precision(int prec);
     int set_tile(int tile);
     // -1 automatic (default); 0 one tile per CTA; 1 persistent TMA-pipelined;
-    // 2 persistent strip-split (fast numerics). Falls back where not compiled.
+    // 2 persistent strip-split (fast numerics); 3 z-streaming strips (fast
+    // numerics, separable damping, X a multiple of 4). Falls back where not
+    // compiled or not applicable.
     int set_variant(int variant);
+    // rows per segment of the z-streaming kernels (>= 8)
+    int set_stream_rows(int rows);
     int variant_in_use() const;
     // waits for the stream and reports a timed-out bounded wait in a kernel
     int sync();
@@ -115,6 +120,7 @@ class Engine {
     int capture(cudaGraphExec_t *out, Emit emit);
     int launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, int pin, int ain);
     int launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain, int in1);
+    int launch_stream(const StepParams &p, int kind);  // 0 forward, 1 forward + ring, 2 reverse
     void drop_graphs();
     StepParams base_params() const;
     void free_all();
@@ -178,6 +184,9 @@ class Engine {
     bool ck_valid_ = false;
 
     int variant_ = -1;
+    // z-streaming kernel tables (built with the other tables)
+    StreamTabs stb_{};
+    int n_strips_ = 0, seg_h_ = 64;
     int *derr_ = nullptr;         // device error flag of the bounded waits
     TmaParams *tmap_ = nullptr;   // tensor maps of every field, slot and coefficient
     bool maps_dirty_ = true;

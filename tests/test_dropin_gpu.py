@@ -143,6 +143,28 @@ def test_strip_split_kernels_close_to_oracle(lib, tile):
         _assert_close(res, ref, 1e-4, 1e-3, f"split vs split-field fast tile {tile}")
 
 
+@pytest.mark.parametrize("rows", [8, 24, 64, 200])
+def test_streaming_kernels_close_to_oracle(lib, rows):
+    """z-streaming strips (kernel 3) with several segment heights: within the
+    fast-mode tolerance of the FP64 oracle and of the strip-split kernels, on
+    the medium case, the strip case (points inside the damped strips) and a
+    grid wider than two strips whose width is not a multiple of the strip."""
+    import make_sim_golden
+    from otfwi_b200 import scenarios
+    from otfwi_b200.cuda_interface_pml import pml_damping
+    os.environ["OTFWI_STREAM_ROWS"] = str(rows)
+    try:
+        sc = scenarios.small(X=268, Z=84, T=220, n_src=2, n_rec=7, seed=12, f0=0.05)
+        wide = make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))
+        for inp in (_cases()["medium"], _strip_case(), wide):
+            res = _run(lib, inp, precision=1, kernel=3)
+            _assert_close(res, oracle_case(inp, "f64"), 1e-4, 1e-3, f"stream vs oracle f64 rows {rows}")
+            ref = _run(lib, inp, precision=1, tile=4, kernel=2)
+            _assert_close(res, ref, 1e-5, 1e-4, f"stream vs strip-split rows {rows}")
+    finally:
+        os.environ.pop("OTFWI_STREAM_ROWS", None)
+
+
 def test_odd_grid_sizes_every_tile(lib):
     """Grids that are not multiples of any tile shape, both kernel variants."""
     import make_sim_golden
