@@ -19,6 +19,8 @@ LIBDIR = os.path.join(PKG, "lib")
 OBJDIR = os.path.join(PKG, "lib", "obj")
 LIB = os.path.join(LIBDIR, "libotfwi.so")
 DROPIN = os.path.join(LIBDIR, "cuda_regression_PML_single.so")
+# second library: the CPML forward path under the reference's CPML library name
+CPML_LIB = os.path.join(LIBDIR, "cuda_regression_CPML.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--fmad=true",
@@ -36,9 +38,16 @@ def _sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
+def _cpml_sources():
+    d = os.path.join(CSRC, "cpml")
+    return sorted(os.path.join(d, f) for f in os.listdir(d) if f.endswith(".cu")) + \
+        [os.path.join(CSRC, "status.cu")]
+
+
 def _deps():
     out = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     out.append(os.path.join(ROOT, "include", "otfwi.h"))
+    out.append(os.path.join(ROOT, "include", "otfwi_cpml.h"))
     return out
 
 
@@ -49,6 +58,11 @@ def _stale(target, inputs):
     return any(os.path.getmtime(p) > t for p in inputs)
 
 
+def _obj(src):
+    rel = os.path.relpath(src, CSRC).replace(os.sep, "_")
+    return os.path.join(OBJDIR, rel[:-3] + ".o")
+
+
 def build(verbose=False, ptxas_info=False):
     """Compile the library if any source changed; return the library path."""
     os.makedirs(OBJDIR, exist_ok=True)
@@ -56,8 +70,9 @@ def build(verbose=False, ptxas_info=False):
     srcs = _sources()
     deps = _deps()
     jobs = []
-    for s in srcs:
-        obj = os.path.join(OBJDIR, os.path.basename(s)[:-3] + ".o")
+    cpml_srcs = _cpml_sources()
+    for s in sorted(set(srcs) | set(cpml_srcs)):
+        obj = _obj(s)
         if _stale(obj, [s] + deps):
             cmd = [nvcc, "-c", s, "-o", obj, "-I", os.path.join(ROOT, "include")] + NVFLAGS
             if ptxas_info:
@@ -76,7 +91,12 @@ def build(verbose=False, ptxas_info=False):
                     sys.stdout.write(r.stdout + r.stderr)
                 if r.returncode != 0:
                     raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
-    objs = [os.path.join(OBJDIR, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    objs = [_obj(s) for s in srcs]
+    cobjs = [_obj(s) for s in cpml_srcs]
+    if jobs or _stale(CPML_LIB, cobjs):
+        r = subprocess.run([nvcc, "-shared", "-o", CPML_LIB] + cobjs + ARCH, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"CPML link failed:\n{r.stdout}\n{r.stderr}")
     if jobs or _stale(LIB, objs):
         cmd = [nvcc, "-shared", "-o", LIB] + objs + ARCH + ["-lcuda"]
         r = subprocess.run(cmd, capture_output=True, text=True)

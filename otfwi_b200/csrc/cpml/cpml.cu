@@ -1,0 +1,429 @@
+// Second-order acoustic CPML forward path and the reference's CPML C ABI
+// (lib/cuda_regression_CPML.so; the reference builds the same ABI from
+// simulator/src/regression_CPML.cu into bin/cuda_regression_CPML.so).
+//
+// One fused launch per time step replaces the reference's two frame kernels
+// (regression_CPML.cu:49-207): a CTA owns a 32 x 16 tile, stages P(t-1) with
+// an 8-cell halo, computes the first staggered derivatives, their CPML
+// memory variables and the density division on the tile plus a 4-cell halo
+// (halo recomputed, not exchanged), then the second derivatives, their
+// memory variables and P(t) = 2 P(t-1) - P(t-2) + lap dt^2 kappa on the
+// owned cells. Source injection (:210-231) and recording (:238-246) are two
+// small launches after it, as in the reference. Fields keep the reference's
+// layout: P in four time slots [4][Z][X] (so cells outside the update region
+// hold what the reference's would), memory variables of the first
+// derivatives in two slots (the halo recompute reads t-1 while owners write
+// t), those of the second derivatives in place.
+//
+// Numerics: faithful (default) restates the reference's arithmetic: 8-tap
+// staggered sums in FP64 (leading product rounded, seven FMAs), FP32 updates
+// with the contractions fma(b, m, a*v) and fma(lap*dt2, kappa, 2 P1 - P2),
+// IEEE divisions; fast uses the FP32 antisymmetric-pair staggered sums.
+#include <cuda_runtime.h>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "../otf_common.cuh"
+#include "../../../include/otfwi_cpml.h"
+
+namespace otf {
+namespace cpml {
+
+constexpr int TX = 32, TZ = 16, NTH = 256;
+constexpr int SW = TX + 16, SH = TZ + 16;  // P(t-1) tile with an 8-cell halo
+constexpr int VW = TX + 8, VH = TZ + 8;    // first-derivative region (4-cell halo)
+
+constexpr double kC0 = 1.196289e+00, kC1 = 7.975260e-02, kC2 = 9.570313e-03, kC3 = 6.975446e-04;
+
+struct Coef {
+    const float *Kx, *ax, *bx, *Kxh, *axh, *bxh;  // [X]
+    const float *Kz, *az, *bz, *Kzh, *azh, *bzh;  // [Z]
+    const float *kappa, *rho_hx, *rho_hz;         // [Z][X]
+    float dx, dz, dt2;
+};
+
+struct StepArgs {
+    int X, Z, t;
+    const float *P1, *P2;  // P(t-1), P(t-2)
+    float *Pn;             // P(t)
+    const float *mx_in, *mz_in;
+    float *mx_out, *mz_out;
+    float *mxx, *mzz;      // in place
+    Coef c;
+};
+
+__device__ __forceinline__ bool inb(int X, int Z, int x, int z) { return x >= 4 && z >= 4 && x < X - 4 && z < Z - 4; }
+
+// derivPMLdx / dz (deriv_macros.h:85-108) from w[0..7] = m[c-3-off .. c+4-off]
+template <bool FAITHFUL>
+__device__ __forceinline__ float stag(const float *w, int stride)
+{
+    if (FAITHFUL) {
+        double s = -kC3 * (double)w[7 * stride];
+        s = fma(kC2, (double)w[6 * stride], s);
+        s = fma(-kC1, (double)w[5 * stride], s);
+        s = fma(kC0, (double)w[4 * stride], s);
+        s = fma(-kC0, (double)w[3 * stride], s);
+        s = fma(kC1, (double)w[2 * stride], s);
+        s = fma(-kC2, (double)w[1 * stride], s);
+        s = fma(kC3, (double)w[0], s);
+        return (float)s;
+    } else {
+        constexpr float c0h = (float)kC0, c0l = (float)(kC0 - (double)(float)kC0);
+        const float d0 = __fsub_rn(w[4 * stride], w[3 * stride]);
+        const float d1 = __fsub_rn(w[5 * stride], w[2 * stride]);
+        const float d2 = __fsub_rn(w[6 * stride], w[1 * stride]);
+        const float d3 = __fsub_rn(w[7 * stride], w[0]);
+        float s = __fmul_rn(-(float)kC3, d3);
+        s = __fmaf_rn((float)kC2, d2, s);
+        s = __fmaf_rn(-(float)kC1, d1, s);
+        s = __fmaf_rn(c0l, d0, s);
+        return __fmaf_rn(c0h, d0, s);
+    }
+}
+
+template <bool FAITHFUL>
+__global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
+{
+    __shared__ float sP[SH][SW];
+    __shared__ float sVx[VH][VW], sVz[VH][VW];
+    const int X = a.X, Z = a.Z;
+    const int x0 = blockIdx.x * TX, z0 = blockIdx.y * TZ;
+    for (int k = threadIdx.x; k < SW * SH; k += NTH) {
+        const int zz = k / SW, xx = k - zz * SW;
+        const int x = x0 - 8 + xx, z = z0 - 8 + zz;
+        sP[zz][xx] = inb(X, Z, x, z) ? a.P1[(size_t)z * X + x] : 0.f;
+    }
+    __syncthreads();
+    // first derivatives, memory variables and density division on the tile + 4-cell halo
+    for (int k = threadIdx.x; k < VW * VH; k += NTH) {
+        const int ez = k / VW, ex = k - ez * VW;
+        const int x = x0 - 4 + ex, z = z0 - 4 + ez;
+        float vx = 0.f, vz = 0.f;
+        if (inb(X, Z, x, z)) {
+            const size_t i = (size_t)z * X + x;
+            // offset 0: taps x-3 .. x+4 (tile column of x is ex + 4)
+            const float v0x = __fdiv_rn(stag<FAITHFUL>(&sP[ez + 4][ex + 1], 1), a.c.dx);
+            const float mx = __fmaf_rn(a.c.bxh[x], a.mx_in[i], __fmul_rn(a.c.axh[x], v0x));
+            vx = __fdiv_rn(__fadd_rn(__fdiv_rn(v0x, a.c.Kxh[x]), mx), a.c.rho_hx[i]);
+            const float v0z = __fdiv_rn(stag<FAITHFUL>(&sP[ez + 1][ex + 4], SW), a.c.dz);
+            const float mz = __fmaf_rn(a.c.bzh[z], a.mz_in[i], __fmul_rn(a.c.azh[z], v0z));
+            vz = __fdiv_rn(__fadd_rn(__fdiv_rn(v0z, a.c.Kzh[z]), mz), a.c.rho_hz[i]);
+            if (ex >= 4 && ex < TX + 4 && ez >= 4 && ez < TZ + 4) {
+                a.mx_out[i] = mx;
+                a.mz_out[i] = mz;
+            }
+        }
+        sVx[ez][ex] = vx;
+        sVz[ez][ex] = vz;
+    }
+    __syncthreads();
+    // second derivatives, memory variables and P(t) on the owned cells
+    for (int k = threadIdx.x; k < TX * TZ; k += NTH) {
+        const int oz = k / TX, ox = k - oz * TX;
+        const int x = x0 + ox, z = z0 + oz;
+        if (!inb(X, Z, x, z))
+            continue;
+        const size_t i = (size_t)z * X + x;
+        // offset 1: taps x-4 .. x+3 (region column of x is ox + 4)
+        const float vxx0 = __fdiv_rn(stag<FAITHFUL>(&sVx[oz + 4][ox], 1), a.c.dx);
+        const float mxx = __fmaf_rn(a.c.bx[x], a.mxx[i], __fmul_rn(a.c.ax[x], vxx0));
+        a.mxx[i] = mxx;
+        const float vxx1 = __fadd_rn(__fdiv_rn(vxx0, a.c.Kx[x]), mxx);
+        const float vzz0 = __fdiv_rn(stag<FAITHFUL>(&sVz[oz][ox + 4], VW), a.c.dz);
+        const float mzz = __fmaf_rn(a.c.bz[z], a.mzz[i], __fmul_rn(a.c.az[z], vzz0));
+        a.mzz[i] = mzz;
+        const float vzz1 = __fadd_rn(__fdiv_rn(vzz0, a.c.Kz[z]), mzz);
+        const float lap = __fadd_rn(vxx1, vzz1);
+        a.Pn[i] = __fmaf_rn(__fmul_rn(lap, a.c.dt2), a.c.kappa[i], __fmaf_rn(2.f, a.P1[i], -a.P2[i]));
+    }
+}
+
+// somaFonte (regression_CPML.cu:210-231): P += 4pi c^2 s(t) dt^2; with one
+// pixel per element only source idx fires (all when idx == -1), otherwise
+// every source fires.
+__global__ void k_cpml_source(float *Pn, int X, int T, int t, int ns, int ppe, int idx, const int *sx,
+                              const int *sz, const float *cquad, const float *src, float qtpi, float dt2)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ns || (ppe == 1 && idx != -1 && idx != n))
+        return;
+    const size_t i = (size_t)sz[n] * X + sx[n];
+    const float s = __fmul_rn(__fmul_rn(qtpi, cquad[i]), src[(size_t)n * T + t]);
+    Pn[i] = __fmaf_rn(s, dt2, Pn[i]);
+}
+
+// gravaBufferSensores2ordem (regression_CPML.cu:238-246)
+__global__ void k_cpml_record(const float *Pn, int X, int T, int t, int nm, const int *mx, const int *mz,
+                              float *rec)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < nm)
+        rec[(size_t)n * T + t] = Pn[(size_t)mz[n] * X + mx[n]];
+}
+
+struct State {
+    int X = 0, Z = 0, T = 0, ns = 0, nm = 0, ppe = 1;
+    float dx = 1.f, dz = 1.f, dt = 1.f, dt2 = 1.f, qtpi = 1.f;
+    int precision = 0;
+    cudaStream_t st = nullptr;
+    float *P = nullptr, *mx = nullptr, *mz = nullptr, *mxx = nullptr, *mzz = nullptr;
+    float *cquad = nullptr, *kappa = nullptr, *rho_hx = nullptr, *rho_hz = nullptr;
+    float *cx = nullptr;  // K a b, K_half a_half b_half along x: [6][X]
+    float *cz = nullptr;  // the same along z: [6][Z]
+    float *src = nullptr, *init = nullptr, *rec_d = nullptr, *rec_h = nullptr;
+    int *sx = nullptr, *sz = nullptr, *pmx = nullptr, *pmz = nullptr;
+    int cap_src = 0;
+
+    void release()
+    {
+        float *f[] = {P, mx, mz, mxx, mzz, cquad, kappa, rho_hx, rho_hz, cx, cz, src, init, rec_d};
+        for (float *p : f)
+            if (p)
+                cudaFree(p);
+        int *ip[] = {sx, sz, pmx, pmz};
+        for (int *p : ip)
+            if (p)
+                cudaFree(p);
+        if (rec_h)
+            cudaFreeHost(rec_h);
+        if (st)
+            cudaStreamDestroy(st);
+        *this = State();
+        (void)cudaGetLastError();
+    }
+};
+
+static State g;
+
+static int env_int(const char *name, int dflt)
+{
+    const char *v = std::getenv(name);
+    return v && *v ? std::atoi(v) : dflt;
+}
+
+static bool valid_points(int n, const int *x, const int *z, int X, int Z, bool interior)
+{
+    for (int k = 0; k < n; k++) {
+        if (x[k] < 0 || z[k] < 0 || x[k] >= X || z[k] >= Z)
+            return false;
+        if (interior && !(x[k] >= 4 && z[k] >= 4 && x[k] < X - 4 && z[k] < Z - 4))
+            return false;
+    }
+    return true;
+}
+
+static int init(int X, int Z, int T, int ns, int nm, int ppe, const int *ps_x, const int *ps_z, const int *pm_x,
+                const int *pm_z, float dx, float dz, float dt, float dt2, float qtpi, const float *cq,
+                const float *kp, const float *rhx, const float *rhz, const float *const *cx6,
+                const float *const *cz6, const float *src, const float *init_h)
+{
+    g.release();
+    clear_error();
+    OTF_CHECK(X >= 9 && Z >= 9 && T >= 1, 1, "cpml init_memory_sim: grid or T too small");
+    OTF_CHECK(ns >= 0 && nm >= 0, 1, "cpml init_memory_sim: negative point count");
+    OTF_CHECK(valid_points(ns, ps_x, ps_z, X, Z, true), 1,
+              "cpml init_memory_sim: sources must lie in 4 <= x < X-4, 4 <= z < Z-4");
+    OTF_CHECK(valid_points(nm, pm_x, pm_z, X, Z, false), 1, "cpml init_memory_sim: receiver outside the grid");
+    g.X = X;
+    g.Z = Z;
+    g.T = T;
+    g.ns = ns;
+    g.nm = nm;
+    g.ppe = ppe;
+    g.dx = dx;
+    g.dz = dz;
+    g.dt = dt;
+    g.dt2 = dt2;
+    g.qtpi = qtpi;
+    g.precision = env_int("OTFWI_PRECISION", 0);
+    const size_t XZ = (size_t)X * Z;
+    OTF_CUDA(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+    OTF_CUDA(cudaMalloc(&g.P, 4 * XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.mx, 2 * XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.mz, 2 * XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.mxx, XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.mzz, XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.cquad, XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.kappa, XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.rho_hx, XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.rho_hz, XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.cx, 6 * (size_t)X * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.cz, 6 * (size_t)Z * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.init, 2 * XZ * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.rec_d, std::max<size_t>(1, (size_t)nm * T) * sizeof(float)));
+    OTF_CUDA(cudaMallocHost(&g.rec_h, std::max<size_t>(1, (size_t)nm * T) * sizeof(float)));
+    g.cap_src = std::max(ns, 1);
+    OTF_CUDA(cudaMalloc(&g.src, (size_t)g.cap_src * T * sizeof(float)));
+    OTF_CUDA(cudaMalloc(&g.sx, g.cap_src * sizeof(int)));
+    OTF_CUDA(cudaMalloc(&g.sz, g.cap_src * sizeof(int)));
+    OTF_CUDA(cudaMalloc(&g.pmx, std::max(nm, 1) * sizeof(int)));
+    OTF_CUDA(cudaMalloc(&g.pmz, std::max(nm, 1) * sizeof(int)));
+    OTF_CUDA(cudaMemcpy(g.cquad, cq, XZ * sizeof(float), cudaMemcpyHostToDevice));
+    OTF_CUDA(cudaMemcpy(g.kappa, kp, XZ * sizeof(float), cudaMemcpyHostToDevice));
+    OTF_CUDA(cudaMemcpy(g.rho_hx, rhx, XZ * sizeof(float), cudaMemcpyHostToDevice));
+    OTF_CUDA(cudaMemcpy(g.rho_hz, rhz, XZ * sizeof(float), cudaMemcpyHostToDevice));
+    for (int k = 0; k < 6; k++) {
+        OTF_CUDA(cudaMemcpy(g.cx + (size_t)k * X, cx6[k], X * sizeof(float), cudaMemcpyHostToDevice));
+        OTF_CUDA(cudaMemcpy(g.cz + (size_t)k * Z, cz6[k], Z * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    if (ns > 0) {
+        OTF_CUDA(cudaMemcpy(g.src, src, (size_t)ns * T * sizeof(float), cudaMemcpyHostToDevice));
+        OTF_CUDA(cudaMemcpy(g.sx, ps_x, ns * sizeof(int), cudaMemcpyHostToDevice));
+        OTF_CUDA(cudaMemcpy(g.sz, ps_z, ns * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    if (nm > 0) {
+        OTF_CUDA(cudaMemcpy(g.pmx, pm_x, nm * sizeof(int), cudaMemcpyHostToDevice));
+        OTF_CUDA(cudaMemcpy(g.pmz, pm_z, nm * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    if (init_h)
+        OTF_CUDA(cudaMemcpy(g.init, init_h, 2 * XZ * sizeof(float), cudaMemcpyHostToDevice));
+    else
+        OTF_CUDA(cudaMemset(g.init, 0, 2 * XZ * sizeof(float)));
+    return 0;
+}
+
+static int simulate(int idx)
+{
+    OTF_CHECK(g.P != nullptr, 2, "cpml cuda_simulate2 called before init_memory_sim");
+    const int X = g.X, Z = g.Z, T = g.T;
+    const size_t XZ = (size_t)X * Z;
+    cudaStream_t st = g.st;
+    OTF_CUDA(cudaMemsetAsync(g.P, 0, 4 * XZ * sizeof(float), st));
+    OTF_CUDA(cudaMemcpyAsync(g.P, g.init, 2 * XZ * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    OTF_CUDA(cudaMemsetAsync(g.mx, 0, 2 * XZ * sizeof(float), st));
+    OTF_CUDA(cudaMemsetAsync(g.mz, 0, 2 * XZ * sizeof(float), st));
+    OTF_CUDA(cudaMemsetAsync(g.mxx, 0, XZ * sizeof(float), st));
+    OTF_CUDA(cudaMemsetAsync(g.mzz, 0, XZ * sizeof(float), st));
+    StepArgs a;
+    a.X = X;
+    a.Z = Z;
+    a.c.Kx = g.cx;
+    a.c.ax = g.cx + X;
+    a.c.bx = g.cx + 2 * X;
+    a.c.Kxh = g.cx + 3 * X;
+    a.c.axh = g.cx + 4 * X;
+    a.c.bxh = g.cx + 5 * X;
+    a.c.Kz = g.cz;
+    a.c.az = g.cz + Z;
+    a.c.bz = g.cz + 2 * Z;
+    a.c.Kzh = g.cz + 3 * Z;
+    a.c.azh = g.cz + 4 * Z;
+    a.c.bzh = g.cz + 5 * Z;
+    a.c.kappa = g.kappa;
+    a.c.rho_hx = g.rho_hx;
+    a.c.rho_hz = g.rho_hz;
+    a.c.dx = g.dx;
+    a.c.dz = g.dz;
+    a.c.dt2 = g.dt2;
+    a.mxx = g.mxx;
+    a.mzz = g.mzz;
+    const dim3 grid((X + TX - 1) / TX, (Z + TZ - 1) / TZ);
+    for (int t = 0; t < T; t++) {
+        float *Pn = g.P + (size_t)(t % 4) * XZ;
+        if (t > 1) {
+            a.t = t;
+            a.P1 = g.P + (size_t)((t + 3) % 4) * XZ;
+            a.P2 = g.P + (size_t)((t + 2) % 4) * XZ;
+            a.Pn = Pn;
+            a.mx_in = g.mx + (size_t)((t + 1) % 2) * XZ;
+            a.mz_in = g.mz + (size_t)((t + 1) % 2) * XZ;
+            a.mx_out = g.mx + (size_t)(t % 2) * XZ;
+            a.mz_out = g.mz + (size_t)(t % 2) * XZ;
+            if (g.precision == 1)
+                k_cpml_step<false><<<grid, NTH, 0, st>>>(a);
+            else
+                k_cpml_step<true><<<grid, NTH, 0, st>>>(a);
+            if (g.ns > 0)
+                k_cpml_source<<<(g.ns + 127) / 128, 128, 0, st>>>(Pn, X, T, t, g.ns, g.ppe, idx, g.sx, g.sz,
+                                                                 g.cquad, g.src, g.qtpi, g.dt2);
+        }
+        if (g.nm > 0)
+            k_cpml_record<<<(g.nm + 127) / 128, 128, 0, st>>>(Pn, X, T, t, g.nm, g.pmx, g.pmz, g.rec_d);
+    }
+    OTF_CUDA(cudaGetLastError());
+    if (g.nm > 0)
+        OTF_CUDA(cudaMemcpyAsync(g.rec_h, g.rec_d, (size_t)g.nm * T * sizeof(float), cudaMemcpyDeviceToHost, st));
+    OTF_CUDA(cudaStreamSynchronize(st));
+    return 0;
+}
+
+}  // namespace cpml
+}  // namespace otf
+
+using otf::cpml::g;
+
+extern "C" {
+
+void def_python_adj(void *fn) { (void)fn; }
+
+void init_memory_sim(int x, int z, int t, int ns, int nm, int ppe, int *ps_x, int *ps_z, int *pm_x, int *pm_z,
+                     float dx_h, float dz_h, float dt_h, float dt2_h, float qtpi_h, float *cq, float *kp_unr,
+                     float *rho_h, float *rho_hx_h, float *rho_hz_h, float *d_x_h, float *K_x_h,
+                     float *alpha_x_h, float *a_x_h, float *b_x_h, float *d_x_half_h, float *K_x_half_h,
+                     float *alpha_x_half_h, float *a_x_half_h, float *b_x_half_h, float *d_z_h, float *K_z_h,
+                     float *alpha_z_h, float *a_z_h, float *b_z_h, float *d_z_half_h, float *K_z_half_h,
+                     float *alpha_z_half_h, float *a_z_half_h, float *b_z_half_h, float *src, float *init,
+                     float **rec)
+{
+    (void)rho_h;
+    (void)d_x_h;
+    (void)alpha_x_h;
+    (void)d_x_half_h;
+    (void)alpha_x_half_h;
+    (void)d_z_h;
+    (void)alpha_z_h;
+    (void)d_z_half_h;
+    (void)alpha_z_half_h;
+    const float *cx6[6] = {K_x_h, a_x_h, b_x_h, K_x_half_h, a_x_half_h, b_x_half_h};
+    const float *cz6[6] = {K_z_h, a_z_h, b_z_h, K_z_half_h, a_z_half_h, b_z_half_h};
+    if (otf::cpml::init(x, z, t, ns, nm, ppe, ps_x, ps_z, pm_x, pm_z, dx_h, dz_h, dt_h, dt2_h, qtpi_h, cq, kp_unr,
+                        rho_hx_h, rho_hz_h, cx6, cz6, src, init) == 0 &&
+        rec)
+        *rec = g.rec_h;
+}
+
+void setCquad(float *cq)
+{
+    if (!g.cquad) {
+        otf::set_error_msg(2, "cpml setCquad called before init_memory_sim");
+        return;
+    }
+    const cudaError_t e = cudaMemcpy(g.cquad, cq, (size_t)g.X * g.Z * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess)
+        otf::set_error((int)e, "cpml setCquad", __FILE__, __LINE__);
+}
+
+void set_source(int ns, int *ps_x, int *ps_z)
+{
+    if (!g.sx) {
+        otf::set_error_msg(2, "cpml set_source called before init_memory_sim");
+        return;
+    }
+    if (ns < 0 || ns > g.cap_src) {
+        otf::set_error_msg(1, "cpml set_source: more sources than init_memory_sim allocated waveforms for");
+        return;
+    }
+    if (!otf::cpml::valid_points(ns, ps_x, ps_z, g.X, g.Z, true)) {
+        otf::set_error_msg(1, "cpml set_source: sources must lie in 4 <= x < X-4, 4 <= z < Z-4");
+        return;
+    }
+    g.ns = ns;
+    if (ns > 0 && (cudaMemcpy(g.sx, ps_x, ns * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+                   cudaMemcpy(g.sz, ps_z, ns * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess))
+        otf::set_error_msg(2, "cpml set_source: copy failed");
+}
+
+void cuda_simulate2(int en_out, int idx_source)
+{
+    (void)en_out;
+    otf::cpml::simulate(idx_source);
+}
+
+int otf_last_status(void) { return otf::last_status(); }
+const char *otf_last_error(void) { return otf::last_error(); }
+void otf_clear_error(void) { otf::clear_error(); }
+void otf_cpml_release(void) { g.release(); }
+
+}  // extern "C"

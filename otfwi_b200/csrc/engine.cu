@@ -13,31 +13,6 @@ namespace otf {
 
 const TileShape kTileShapes[kNumTileShapes] = {{56, 56}, {120, 24}, {120, 56}, {248, 24}, {56, 24}};
 
-// ---------------------------------------------------------------- errors
-static thread_local int g_status = 0;
-static thread_local std::string g_msg;
-
-void set_error(int code, const char *what, const char *file, int line)
-{
-    g_status = code ? code : -1;
-    char buf[512];
-    snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what,
-             cudaGetErrorString((cudaError_t)code), file, line);
-    g_msg = buf;
-}
-void set_error_msg(int code, const std::string &msg)
-{
-    g_status = code ? code : -1;
-    g_msg = msg;
-}
-void clear_error()
-{
-    g_status = 0;
-    g_msg.clear();
-}
-int last_status() { return g_status; }
-const char *last_error() { return g_msg.c_str(); }
-
 // ---------------------------------------------------------- helper kernels
 
 // Running integral of each row (somaFonteIntegral's "integral[n] +=",

@@ -1,0 +1,68 @@
+"""CPU tests of the CPML path: the library exports every symbol its header
+declares, the profiles are the convolutional-PML recursion coefficients,
+and the oracle's reference-arithmetic mode agrees with its FP64 mode."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import cpml_oracle as co
+from conftest import ROOT
+
+
+def test_cpml_library_exports_header_symbols():
+    from otfwi_b200 import _lib
+    from otfwi_b200.cpml import CPML_LIB
+    if not os.path.exists(CPML_LIB):
+        pytest.skip("CPML library not built")
+    L = ctypes.CDLL(CPML_LIB)
+    names = _lib.exported_symbols_from_header(os.path.join(ROOT, "include", "otfwi_cpml.h"))
+    for ref_name in ("init_memory_sim", "setCquad", "set_source", "cuda_simulate2", "def_python_adj"):
+        assert ref_name in names
+    assert not [n for n in names if not hasattr(L, n)]
+
+
+def test_profiles_are_the_cpml_recursion():
+    from otfwi_b200.cpml import cpml_profiles
+    (d, K, al, a, b), (dh, Kh, alh, ah, bh) = cpml_profiles(100, 20, 1.0, 0.5, 0.4, 0.05)
+    inner = slice(21, 79)
+    assert np.all(d[inner] == 0) and np.all(a[inner] == 0) and np.all(b[inner] == 1)
+    assert d[0] > d[10] > 0 and d[-1] > d[-10] > 0
+    assert np.allclose(b, np.exp(-(d / K + al) * 0.5), rtol=1e-6)
+    m = d > 0
+    assert np.allclose(a[m], d[m] * (b[m] - 1) / (K[m] * (d[m] + K[m] * al[m])), rtol=1e-5)
+    assert np.all(dh[:19] > 0) and dh[50] == 0
+
+
+def _inputs(X=72, Z=64, T=250):
+    """Arrays as CPMLSimulator passes them, built without a library."""
+    from otfwi_b200 import scenarios
+    from otfwi_b200.cpml import cpml_profiles
+    sc = scenarios.small(X=X, Z=Z, T=T, n_src=2, n_rec=5, seed=11, f0=0.05)
+    c = sc.c_true.astype(np.float64)
+    f32 = lambda a: np.ascontiguousarray(np.asarray(a, np.float32).ravel())
+    i32 = lambda a: np.ascontiguousarray(np.asarray(a, np.int32).ravel())
+    sz, sx = np.where(sc.src_mask)
+    mz, mx = np.where(sc.rec_mask)
+    inp = {"ps_x": i32(sx), "ps_z": i32(sz), "pm_x": i32(mx), "pm_z": i32(mz), "cq": f32(c * c),
+           "kappa": f32(c * c), "rhx": f32(np.ones((Z, X))), "rhz": f32(np.ones((Z, X))), "src": f32(sc.source),
+           "init": f32(np.zeros((2, Z, X)))}
+    for name, prof in zip(("x", "xh"), cpml_profiles(X, sc.PML, 1.0, 1.0, float(c.max()), 0.05)):
+        for k, v in zip(("d", "K", "alpha", "a", "b"), prof):
+            inp[f"{k}_{name}"] = f32(v)
+    for name, prof in zip(("z", "zh"), cpml_profiles(Z, sc.PML, 1.0, 1.0, float(c.max()), 0.05)):
+        for k, v in zip(("d", "K", "alpha", "a", "b"), prof):
+            inp[f"{k}_{name}"] = f32(v)
+    return inp, X, Z, T
+
+
+def test_cpml_oracle_modes_agree_and_absorb():
+    inp, X, Z, T = _inputs()
+    r32 = co.simulate(inp, X, Z, T)
+    r64 = co.simulate(inp, X, Z, T, mode="f64")
+    assert np.abs(r64).max() > 0
+    assert np.abs(r32 - r64).max() <= 1e-5 * np.abs(r64).max()
+    # the layers absorb: the late traces are far below the direct arrival
+    late = np.abs(r64[:, -40:]).max()
+    assert late < 0.05 * np.abs(r64).max()

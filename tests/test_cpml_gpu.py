@@ -1,0 +1,70 @@
+"""GPU tests of the second-order CPML library (lib/cuda_regression_CPML.so)
+against the reference's own CPML library outputs (tests/golden/cpml_*.npz,
+made by tests/golden/make_cpml_golden.py) and the CPU oracle.
+
+Tolerances: faithful numerics bit-identical to the reference library and to
+the oracle's reference-arithmetic mode; against the FP64 oracle max|d| /
+max|ref| <= 1e-5 (faithful) and 1e-4 (fast FP32 staggered sums)."""
+import glob
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import cpml_oracle as co
+from conftest import GOLDEN, ROOT
+
+pytestmark = pytest.mark.gpu
+
+sys.path.insert(0, GOLDEN)
+
+
+def _ours(name, precision=0):
+    """Traces of this package's CPML library for a golden case, in a child
+    process (the drop-in keeps process-global state)."""
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r); sys.path.insert(0, %r);"
+        "import make_cpml_golden as m; sim, idx, ppe = m.case_sim(%r, None);"
+        "np.save(sys.argv[1], sim.simulate(idx))" % (ROOT, GOLDEN, name))
+    out = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"cpml_{name}_{precision}_{os.getpid()}.npy")
+    env = dict(os.environ, OTFWI_PRECISION=str(precision))
+    subprocess.run([sys.executable, "-c", code, out], check=True, env=env)
+    r = np.load(out)
+    os.remove(out)
+    return r
+
+
+def _rel(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "cpml_*.npz"))), ids=os.path.basename)
+def test_cpml_matches_reference_library_and_oracle(path):
+    d = np.load(path)
+    name = os.path.basename(path)[:-4]
+    X, Z, T, idx, ppe = (int(d[k]) for k in ("X", "Z", "T", "idx", "ppe"))
+    inp = {k: d[k] for k in d.files}
+    ours = _ours(name)
+    nd = int(np.sum(ours != d["traces"]))
+    print(name, "differing samples vs reference library:", nd, "max rel", _rel(ours, d["traces"]))
+    assert nd == 0
+    o32 = co.simulate(inp, X, Z, T, idx_source=idx, ppe=ppe)
+    assert np.array_equal(o32, d["traces"])  # the oracle pinned to the reference
+    o64 = co.simulate(inp, X, Z, T, idx_source=idx, ppe=ppe, mode="f64")
+    assert _rel(ours, o64) <= 1e-5
+    fast = _ours(name, precision=1)
+    print(name, "fast vs FP64 oracle", _rel(fast, o64))
+    assert _rel(fast, o64) <= 1e-4
+
+
+def test_cpml_errors_are_reported():
+    from otfwi_b200 import _lib
+    from otfwi_b200.cpml import CPMLSimulator
+    from otfwi_b200 import scenarios
+    sc = scenarios.small(X=64, Z=64, T=50, n_src=1, n_rec=2, seed=1)
+    sc.src_mask[:] = False
+    sc.src_mask[2, 30] = True  # z = 2: outside the update region
+    with pytest.raises(_lib.OtfwiError):
+        CPMLSimulator(sc.X, sc.Z, sc.T, sc.PML, sc.c_true, sc.src_mask, sc.rec_mask, sc.source)
