@@ -51,6 +51,14 @@ void set_source(int ns, int *ps_x, int *ps_z);
  * of every receiver from t = 0 into the buffer returned by init_memory_sim. */
 void cuda_simulate2(int en_out, int idx_source);
 
+/* Exact discrete adjoint of the forward map (no counterpart in the
+ * reference, which has no CPML gradient): grad_kappa [Z*X] = dL/dkappa for
+ * dL/dtraces = g [nm*T] (host arrays), kappa = rho c^2 the Laplacian's
+ * coefficient (the source term's c^2 held fixed). The forward is recomputed
+ * with the state kept every checkpoint_every steps (sqrt(T) minimises
+ * memory). Returns 0, or -1 with otf_last_error set. */
+int otf_cpml_gradient(const float *g, float *grad_kappa, int checkpoint_every, int idx_source);
+
 /* Status (additive; no reference counterpart) and release of every buffer. */
 int otf_last_status(void);
 const char *otf_last_error(void);

@@ -9,7 +9,8 @@ that caller: ``cpml_profiles`` builds the d, K, alpha, a, b profiles at the
 integer and half points (the unsplit convolutional PML recursion
 b = exp(-(d/K + alpha) dt), a = d (b - 1) / (K (d + K alpha))), and
 ``CPMLSimulator`` drives any library with this ABI -- this package's
-lib/cuda_regression_CPML.so by default.
+lib/cuda_regression_CPML.so by default, which adds the exact discrete
+adjoint (``CPMLSimulator.gradient``: dL/dkappa, no reference counterpart).
 """
 import ctypes
 import os
@@ -61,6 +62,9 @@ def _declare(L):
     L.set_source.argtypes = [c_int, ip, ip]
     L.cuda_simulate2.restype = None
     L.cuda_simulate2.argtypes = [c_int, c_int]
+    if hasattr(L, "otf_cpml_gradient"):
+        L.otf_cpml_gradient.restype = c_int
+        L.otf_cpml_gradient.argtypes = [fp, fp, c_int, c_int]
     L._cpml_declared = True
     return L
 
@@ -131,3 +135,18 @@ class CPMLSimulator:
         self._check()
         n = self.n_rec * self.T
         return np.ctypeslib.as_array(self._rec, shape=(n,)).copy().reshape(self.n_rec, self.T)
+
+    def gradient(self, g, idx_source=-1, checkpoint_every=None):
+        """dL/dkappa [Z, X] for dL/dtraces = g [n_rec, T] (exact discrete
+        adjoint of the forward; this package's library only)."""
+        if not hasattr(self.L, "otf_cpml_gradient"):
+            raise _lib.OtfwiError("this CPML library has no gradient")
+        every = checkpoint_every or max(1, int(np.ceil(np.sqrt(self.T))))
+        gg = np.ascontiguousarray(np.asarray(g, np.float32).reshape(self.n_rec, self.T))
+        out = np.zeros((self.Z, self.X), np.float32)
+        rc = self.L.otf_cpml_gradient(gg.ctypes.data_as(POINTER(c_float)), out.ctypes.data_as(POINTER(c_float)),
+                                      int(every), int(idx_source))
+        self._check()
+        if rc != 0:
+            raise _lib.OtfwiError("otf_cpml_gradient failed")
+        return out

@@ -50,6 +50,7 @@ struct StepArgs {
     const float *mx_in, *mz_in;
     float *mx_out, *mz_out;
     float *mxx, *mzz;      // in place
+    float *lap;            // optional: lap(t) of every owned cell (adjoint recompute)
     Coef c;
 };
 
@@ -137,6 +138,8 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
         const float vzz1 = __fadd_rn(__fdiv_rn(vzz0, a.c.Kz[z]), mzz);
         const float lap = __fadd_rn(vxx1, vzz1);
         a.Pn[i] = __fmaf_rn(__fmul_rn(lap, a.c.dt2), a.c.kappa[i], __fmaf_rn(2.f, a.P1[i], -a.P2[i]));
+        if (a.lap)
+            a.lap[i] = lap;
     }
 }
 
@@ -161,6 +164,101 @@ __global__ void k_cpml_record(const float *Pn, int X, int T, int t, int nm, cons
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n < nm)
         rec[(size_t)n * T + t] = Pn[(size_t)mz[n] * X + mx[n]];
+}
+
+// ---- exact discrete adjoint (dL/dkappa), the transposed step in three passes.
+// W[k + 3], k = -3..4: weight of m[c + k - off] in derivPMLdx(m, off, c).
+__constant__ float kW[8] = {(float)kC3, -(float)kC2, (float)kC1, -(float)kC0,
+                            (float)kC0, -(float)kC1, (float)kC2, -(float)kC3};
+
+// transpose of the staggered gather: sum_k W[k+3] a[j - (k - off) d] over inbounds sources
+__device__ __forceinline__ float stagT(const float *a, int X, int Z, int x, int z, int ddx, int ddz, int off)
+{
+    float s = 0.f;
+#pragma unroll
+    for (int k = -3; k <= 4; k++) {
+        const int xx = x - (k - off) * ddx, zz = z - (k - off) * ddz;
+        if (inb(X, Z, xx, zz))
+            s = fmaf(kW[k + 3], a[(size_t)zz * X + xx], s);
+    }
+    return s;
+}
+
+struct AdjArgs {
+    int X, Z;
+    float *LA, *LB, *LC;            // adjoint of P(t), partial adjoints of P(t-1), P(t-2)
+    float *lmx, *lmz, *lmxx, *lmzz; // adjoints carried by the memory variables
+    float *a0x, *a0z, *l0x, *l0z;   // adjoints of the second / first derivatives
+    const float *lap;               // lap(t)
+    float *grad;                    // dL/dkappa
+    Coef c;
+};
+
+// P(t) = 2 P(t-1) - P(t-2) + dt2 kappa (vxx0/Kx + mxx(t) + vzz0/Kz + mzz(t))
+__global__ void k_cpml_adj_a(const AdjArgs a)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)a.X * a.Z)
+        return;
+    const int z = (int)(i / a.X), x = (int)(i - (int64_t)z * a.X);
+    if (!inb(a.X, a.Z, x, z)) {
+        a.a0x[i] = a.a0z[i] = 0.f;
+        a.LC[i] = 0.f;
+        return;
+    }
+    const float la = a.LA[i];
+    a.grad[i] = fmaf(la * a.c.dt2, a.lap[i], a.grad[i]);
+    const float gl = a.c.dt2 * a.c.kappa[i] * la;
+    a.LB[i] = fmaf(2.f, la, a.LB[i]);
+    a.LC[i] = -la;
+    const float tx = a.lmxx[i] + gl;
+    a.a0x[i] = gl / a.c.Kx[x] + a.c.ax[x] * tx;
+    a.lmxx[i] = a.c.bx[x] * tx;
+    const float tz = a.lmzz[i] + gl;
+    a.a0z[i] = gl / a.c.Kz[z] + a.c.az[z] * tz;
+    a.lmzz[i] = a.c.bz[z] * tz;
+}
+
+// vxx0 = D(v1x, off 1)/dx; v1x = (v0x/Kxh + mx(t))/rho_hx, mx(t) = bxh mx(t-1) + axh v0x
+__global__ void k_cpml_adj_b(const AdjArgs a)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)a.X * a.Z)
+        return;
+    const int z = (int)(i / a.X), x = (int)(i - (int64_t)z * a.X);
+    if (!inb(a.X, a.Z, x, z)) {
+        a.l0x[i] = a.l0z[i] = 0.f;
+        return;
+    }
+    const float lv1x = stagT(a.a0x, a.X, a.Z, x, z, 1, 0, 1) / a.c.dx;
+    const float tx = a.lmx[i] + lv1x / a.c.rho_hx[i];
+    a.l0x[i] = lv1x / (a.c.Kxh[x] * a.c.rho_hx[i]) + a.c.axh[x] * tx;
+    a.lmx[i] = a.c.bxh[x] * tx;
+    const float lv1z = stagT(a.a0z, a.X, a.Z, x, z, 0, 1, 1) / a.c.dz;
+    const float tz = a.lmz[i] + lv1z / a.c.rho_hz[i];
+    a.l0z[i] = lv1z / (a.c.Kzh[z] * a.c.rho_hz[i]) + a.c.azh[z] * tz;
+    a.lmz[i] = a.c.bzh[z] * tz;
+}
+
+// v0x = D(P(t-1), off 0)/dx into the adjoint of P(t-1)
+__global__ void k_cpml_adj_c(const AdjArgs a)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)a.X * a.Z)
+        return;
+    const int z = (int)(i / a.X), x = (int)(i - (int64_t)z * a.X);
+    if (!inb(a.X, a.Z, x, z))
+        return;
+    a.LB[i] += stagT(a.l0x, a.X, a.Z, x, z, 1, 0, 0) / a.c.dx + stagT(a.l0z, a.X, a.Z, x, z, 0, 1, 0) / a.c.dz;
+}
+
+// the loss gradient of the traces at step t enters the adjoint of P(t)
+__global__ void k_cpml_adj_g(float *LA, const float *g, int X, int Z, int T, int t, int nm, const int *mx,
+                             const int *mz)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < nm && inb(X, Z, mx[n], mz[n]))
+        atomicAdd(LA + (size_t)mz[n] * X + mx[n], g[(size_t)n * T + t]);
 }
 
 struct State {
@@ -284,19 +382,9 @@ static int init(int X, int Z, int T, int ns, int nm, int ppe, const int *ps_x, c
     return 0;
 }
 
-static int simulate(int idx)
+static void fill_args(StepArgs &a)
 {
-    OTF_CHECK(g.P != nullptr, 2, "cpml cuda_simulate2 called before init_memory_sim");
-    const int X = g.X, Z = g.Z, T = g.T;
-    const size_t XZ = (size_t)X * Z;
-    cudaStream_t st = g.st;
-    OTF_CUDA(cudaMemsetAsync(g.P, 0, 4 * XZ * sizeof(float), st));
-    OTF_CUDA(cudaMemcpyAsync(g.P, g.init, 2 * XZ * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    OTF_CUDA(cudaMemsetAsync(g.mx, 0, 2 * XZ * sizeof(float), st));
-    OTF_CUDA(cudaMemsetAsync(g.mz, 0, 2 * XZ * sizeof(float), st));
-    OTF_CUDA(cudaMemsetAsync(g.mxx, 0, XZ * sizeof(float), st));
-    OTF_CUDA(cudaMemsetAsync(g.mzz, 0, XZ * sizeof(float), st));
-    StepArgs a;
+    const int X = g.X, Z = g.Z;
     a.X = X;
     a.Z = Z;
     a.c.Kx = g.cx;
@@ -319,34 +407,174 @@ static int simulate(int idx)
     a.c.dt2 = g.dt2;
     a.mxx = g.mxx;
     a.mzz = g.mzz;
-    const dim3 grid((X + TX - 1) / TX, (Z + TZ - 1) / TZ);
+    a.lap = nullptr;
+}
+
+// P(0), P(1) from the initial field, every other slot and memory variable zero
+static int reset_state()
+{
+    const size_t XZ = (size_t)g.X * g.Z;
+    cudaStream_t st = g.st;
+    OTF_CUDA(cudaMemsetAsync(g.P, 0, 4 * XZ * sizeof(float), st));
+    OTF_CUDA(cudaMemcpyAsync(g.P, g.init, 2 * XZ * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    OTF_CUDA(cudaMemsetAsync(g.mx, 0, 2 * XZ * sizeof(float), st));
+    OTF_CUDA(cudaMemsetAsync(g.mz, 0, 2 * XZ * sizeof(float), st));
+    OTF_CUDA(cudaMemsetAsync(g.mxx, 0, XZ * sizeof(float), st));
+    OTF_CUDA(cudaMemsetAsync(g.mzz, 0, XZ * sizeof(float), st));
+    return 0;
+}
+
+// one time step t >= 2: the fused step and the source injection (lap optional)
+static void step(StepArgs &a, int t, int idx, float *lap)
+{
+    const size_t XZ = (size_t)g.X * g.Z;
+    float *Pn = g.P + (size_t)(t % 4) * XZ;
+    a.t = t;
+    a.P1 = g.P + (size_t)((t + 3) % 4) * XZ;
+    a.P2 = g.P + (size_t)((t + 2) % 4) * XZ;
+    a.Pn = Pn;
+    a.mx_in = g.mx + (size_t)((t + 1) % 2) * XZ;
+    a.mz_in = g.mz + (size_t)((t + 1) % 2) * XZ;
+    a.mx_out = g.mx + (size_t)(t % 2) * XZ;
+    a.mz_out = g.mz + (size_t)(t % 2) * XZ;
+    a.lap = lap;
+    const dim3 grid((g.X + TX - 1) / TX, (g.Z + TZ - 1) / TZ);
+    if (g.precision == 1)
+        k_cpml_step<false><<<grid, NTH, 0, g.st>>>(a);
+    else
+        k_cpml_step<true><<<grid, NTH, 0, g.st>>>(a);
+    if (g.ns > 0)
+        k_cpml_source<<<(g.ns + 127) / 128, 128, 0, g.st>>>(Pn, g.X, g.T, t, g.ns, g.ppe, idx, g.sx, g.sz,
+                                                           g.cquad, g.src, g.qtpi, g.dt2);
+}
+
+static int simulate(int idx)
+{
+    OTF_CHECK(g.P != nullptr, 2, "cpml cuda_simulate2 called before init_memory_sim");
+    const int X = g.X, T = g.T;
+    const size_t XZ = (size_t)X * g.Z;
+    cudaStream_t st = g.st;
+    if (reset_state())
+        return -1;
+    StepArgs a;
+    fill_args(a);
     for (int t = 0; t < T; t++) {
-        float *Pn = g.P + (size_t)(t % 4) * XZ;
-        if (t > 1) {
-            a.t = t;
-            a.P1 = g.P + (size_t)((t + 3) % 4) * XZ;
-            a.P2 = g.P + (size_t)((t + 2) % 4) * XZ;
-            a.Pn = Pn;
-            a.mx_in = g.mx + (size_t)((t + 1) % 2) * XZ;
-            a.mz_in = g.mz + (size_t)((t + 1) % 2) * XZ;
-            a.mx_out = g.mx + (size_t)(t % 2) * XZ;
-            a.mz_out = g.mz + (size_t)(t % 2) * XZ;
-            if (g.precision == 1)
-                k_cpml_step<false><<<grid, NTH, 0, st>>>(a);
-            else
-                k_cpml_step<true><<<grid, NTH, 0, st>>>(a);
-            if (g.ns > 0)
-                k_cpml_source<<<(g.ns + 127) / 128, 128, 0, st>>>(Pn, X, T, t, g.ns, g.ppe, idx, g.sx, g.sz,
-                                                                 g.cquad, g.src, g.qtpi, g.dt2);
-        }
+        if (t > 1)
+            step(a, t, idx, nullptr);
         if (g.nm > 0)
-            k_cpml_record<<<(g.nm + 127) / 128, 128, 0, st>>>(Pn, X, T, t, g.nm, g.pmx, g.pmz, g.rec_d);
+            k_cpml_record<<<(g.nm + 127) / 128, 128, 0, st>>>(g.P + (size_t)(t % 4) * XZ, X, T, t, g.nm, g.pmx,
+                                                              g.pmz, g.rec_d);
     }
     OTF_CUDA(cudaGetLastError());
     if (g.nm > 0)
         OTF_CUDA(cudaMemcpyAsync(g.rec_h, g.rec_d, (size_t)g.nm * T * sizeof(float), cudaMemcpyDeviceToHost, st));
     OTF_CUDA(cudaStreamSynchronize(st));
     return 0;
+}
+
+// dL/dkappa of the forward map for dL/dtraces = g_h [nm][T]: forward keeping
+// the full state after steps 1, 1+k, 1+2k, ...; then, per segment from the
+// last, the forward recomputed from its checkpoint keeping lap(t), and the
+// transposed steps backwards. The gradient is the exact adjoint of the
+// forward the library computes (its FP32 Laplacians), summed in FP32.
+static int gradient(int idx, int every, const float *g_h, float *grad_h)
+{
+    OTF_CHECK(g.P != nullptr, 2, "cpml gradient called before init_memory_sim");
+    OTF_CHECK(every >= 1, 1, "cpml gradient: checkpoint interval must be >= 1");
+    OTF_CHECK(g.T >= 3, 1, "cpml gradient: T must be at least 3");
+    const int X = g.X, Z = g.Z, T = g.T;
+    const size_t XZ = (size_t)X * Z;
+    cudaStream_t st = g.st;
+    const int n_ck = (T - 2 + every - 1) / every + 1;  // checkpoints at 1 + j*every <= T-1
+    std::vector<float *> bufs;
+    auto alloc = [&](size_t n, float **p) -> int {
+        OTF_CUDA(cudaMalloc(p, n * sizeof(float)));
+        bufs.push_back(*p);
+        return 0;
+    };
+    auto done = [&](int rc) {
+        for (float *p : bufs)
+            cudaFree(p);
+        return rc;
+    };
+    float *ck, *lapb, *LA, *LB, *LC, *lmx, *lmz, *lmxx, *lmzz, *a0x, *a0z, *l0x, *l0z, *grad, *gd;
+    if (alloc((size_t)n_ck * 6 * XZ, &ck) || alloc((size_t)every * XZ, &lapb) || alloc(XZ, &LA) ||
+        alloc(XZ, &LB) || alloc(XZ, &LC) || alloc(XZ, &lmx) || alloc(XZ, &lmz) || alloc(XZ, &lmxx) ||
+        alloc(XZ, &lmzz) || alloc(XZ, &a0x) || alloc(XZ, &a0z) || alloc(XZ, &l0x) || alloc(XZ, &l0z) ||
+        alloc(XZ, &grad) || alloc(std::max<size_t>(1, (size_t)g.nm * T), &gd))
+        return done(-1);
+    auto save = [&](int j, int c) -> int {
+        float *d = ck + (size_t)j * 6 * XZ;
+        const float *src[6] = {g.P + (size_t)(c % 4) * XZ, g.P + (size_t)((c + 3) % 4) * XZ,
+                               g.mx + (size_t)(c % 2) * XZ, g.mz + (size_t)(c % 2) * XZ, g.mxx, g.mzz};
+        for (int k = 0; k < 6; k++)
+            OTF_CUDA(cudaMemcpyAsync(d + k * XZ, src[k], XZ * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        return 0;
+    };
+    auto restore = [&](int j, int c) -> int {
+        const float *s = ck + (size_t)j * 6 * XZ;
+        float *dst[6] = {g.P + (size_t)(c % 4) * XZ, g.P + (size_t)((c + 3) % 4) * XZ,
+                         g.mx + (size_t)(c % 2) * XZ, g.mz + (size_t)(c % 2) * XZ, g.mxx, g.mzz};
+        for (int k = 0; k < 6; k++)
+            OTF_CUDA(cudaMemcpyAsync(dst[k], s + k * XZ, XZ * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        return 0;
+    };
+    if (reset_state())
+        return done(-1);
+    StepArgs a;
+    fill_args(a);
+    for (int t = 1; t < T; t++) {
+        if (t > 1)
+            step(a, t, idx, nullptr);
+        if ((t - 1) % every == 0 && save((t - 1) / every, t))
+            return done(-1);
+    }
+    if (g.nm > 0)
+        OTF_CUDA(cudaMemcpyAsync(gd, g_h, (size_t)g.nm * T * sizeof(float), cudaMemcpyHostToDevice, st));
+    for (float *p : {LA, LB, LC, lmx, lmz, lmxx, lmzz, grad})
+        OTF_CUDA(cudaMemsetAsync(p, 0, XZ * sizeof(float), st));
+    AdjArgs ad;
+    ad.X = X;
+    ad.Z = Z;
+    ad.lmx = lmx;
+    ad.lmz = lmz;
+    ad.lmxx = lmxx;
+    ad.lmzz = lmzz;
+    ad.a0x = a0x;
+    ad.a0z = a0z;
+    ad.l0x = l0x;
+    ad.l0z = l0z;
+    ad.grad = grad;
+    ad.c = a.c;
+    const unsigned nb = (unsigned)((XZ + 255) / 256);
+    for (int j = n_ck - 1; j >= 0; j--) {
+        const int c = 1 + j * every, end = std::min(c + every, T - 1);
+        if (end <= c)
+            continue;
+        if (restore(j, c))
+            return done(-1);
+        for (int t = c + 1; t <= end; t++)
+            step(a, t, idx, lapb + (size_t)(t - c - 1) * XZ);
+        for (int t = end; t > c; t--) {
+            if (g.nm > 0)
+                k_cpml_adj_g<<<(g.nm + 127) / 128, 128, 0, st>>>(LA, gd, X, Z, T, t, g.nm, g.pmx, g.pmz);
+            ad.LA = LA;
+            ad.LB = LB;
+            ad.LC = LC;
+            ad.lap = lapb + (size_t)(t - c - 1) * XZ;
+            k_cpml_adj_a<<<nb, 256, 0, st>>>(ad);
+            k_cpml_adj_b<<<nb, 256, 0, st>>>(ad);
+            k_cpml_adj_c<<<nb, 256, 0, st>>>(ad);
+            float *tmp = LA;  // P(t-1) becomes the current state
+            LA = LB;
+            LB = LC;
+            LC = tmp;
+        }
+    }
+    OTF_CUDA(cudaGetLastError());
+    OTF_CUDA(cudaMemcpyAsync(grad_h, grad, XZ * sizeof(float), cudaMemcpyDeviceToHost, st));
+    OTF_CUDA(cudaStreamSynchronize(st));
+    return done(0);
 }
 
 }  // namespace cpml
@@ -425,5 +653,11 @@ int otf_last_status(void) { return otf::last_status(); }
 const char *otf_last_error(void) { return otf::last_error(); }
 void otf_clear_error(void) { otf::clear_error(); }
 void otf_cpml_release(void) { g.release(); }
+
+int otf_cpml_gradient(const float *g_traces, float *grad_kappa, int checkpoint_every, int idx_source)
+{
+    otf::clear_error();
+    return otf::cpml::gradient(idx_source, checkpoint_every, g_traces, grad_kappa);
+}
 
 }  // extern "C"
