@@ -55,7 +55,8 @@ def _declare(L):
         return L
     fp, ip = POINTER(c_float), POINTER(c_int)
     L.init_memory_sim.restype = None
-    L.init_memory_sim.argtypes = ([c_int] * 6 + [ip] * 4 + [c_float] * 5 + [fp] * 25 + [POINTER(fp)])
+    # 6 ints, 4 int*, 5 floats, 27 float* (c^2, kappa, 3 densities, 20 profiles, source, initial), float**
+    L.init_memory_sim.argtypes = [c_int] * 6 + [ip] * 4 + [c_float] * 5 + [fp] * 27 + [POINTER(fp)]
     L.setCquad.restype = None
     L.setCquad.argtypes = [fp]
     L.set_source.restype = None

@@ -93,3 +93,22 @@ def test_cpml_adjoint_oracle_matches_finite_differences():
         fd = loss(kp) - loss(km)
         an = float(np.sum(grad.ravel() * (kp.astype(np.float64) - km.astype(np.float64))))
         assert abs(fd - an) <= 1e-5 * abs(fd), (fd, an)
+
+
+def test_cpml_caller_declares_every_abi_argument():
+    """The Python caller's init_memory_sim declaration has exactly the
+    header's (and the reference's) 43 parameters, in the same kinds."""
+    import re
+    from otfwi_b200 import cpml
+    text = open(os.path.join(ROOT, "include", "otfwi_cpml.h")).read()
+    sig = re.search(r"void init_memory_sim\((.*?)\);", text, re.S).group(1)
+    params = [p.strip() for p in sig.split(",")]
+    L = ctypes.CDLL(cpml.CPML_LIB)
+    cpml._declare(L)
+    assert len(L.init_memory_sim.argtypes) == len(params) == 43
+    kinds = ["float**" if "**" in p else ("int*" if p.startswith("int") else "float*") if "*" in p else
+             ("int" if p.startswith("int") else "float") for p in params]
+    for t, k in zip(L.init_memory_sim.argtypes, kinds):
+        name = getattr(t, "__name__", str(t))
+        assert {"int": "c_int", "float": "c_float", "int*": "LP_c_int", "float*": "LP_c_float",
+                "float**": "LP_LP_c_float"}[k] == name, (k, name)
