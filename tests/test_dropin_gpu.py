@@ -156,11 +156,11 @@ def test_streaming_kernels_close_to_oracle(lib, rows):
     try:
         sc = scenarios.small(X=268, Z=84, T=220, n_src=2, n_rec=7, seed=12, f0=0.05)
         wide = make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))
-        for inp in (_cases()["medium"], _strip_case(), wide):
+        for name, inp in (("medium", _cases()["medium"]), ("strip", _strip_case()), ("wide", wide)):
             res = _run(lib, inp, precision=1, kernel=3)
-            _assert_close(res, oracle_case(inp, "f64"), 1e-4, 1e-3, f"stream vs oracle f64 rows {rows}")
+            _assert_close(res, oracle_case(inp, "f64"), 1e-4, 1e-3, f"stream vs oracle f64 {name} rows {rows}")
             ref = _run(lib, inp, precision=1, tile=4, kernel=2)
-            _assert_close(res, ref, 1e-5, 1e-4, f"stream vs strip-split rows {rows}")
+            _assert_close(res, ref, 1e-5, 1e-4, f"stream vs strip-split {name} rows {rows}")
     finally:
         os.environ.pop("OTFWI_STREAM_ROWS", None)
 
