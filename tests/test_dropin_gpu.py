@@ -145,10 +145,14 @@ def test_strip_split_kernels_close_to_oracle(lib, tile):
 
 @pytest.mark.parametrize("rows", [8, 24, 64, 200])
 def test_streaming_kernels_close_to_oracle(lib, rows):
-    """z-streaming strips (kernel 3) with several segment heights: within the
-    fast-mode tolerance of the FP64 oracle and of the strip-split kernels, on
-    the medium case, the strip case (points inside the damped strips) and a
-    grid wider than two strips whose width is not a multiple of the strip."""
+    """z-streaming strips (kernel 3) with several segment heights: on the
+    medium case and the strip case (points inside the damped strips) within
+    the fast-mode tolerance of the FP64 oracle; on these and on a grid wider
+    than two strips whose width is not a multiple of the strip, identical to
+    the strip-split kernels (with dt = dx the two compute the same operations
+    in the same order). On the wide grid some receivers see only numerical
+    precursors within T, so its oracle check is normalised by the largest
+    trace of the shot rather than per receiver."""
     import make_sim_golden
     from otfwi_b200 import scenarios
     from otfwi_b200.cuda_interface_pml import pml_damping
@@ -158,9 +162,15 @@ def test_streaming_kernels_close_to_oracle(lib, rows):
         wide = make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))
         for name, inp in (("medium", _cases()["medium"]), ("strip", _strip_case()), ("wide", wide)):
             res = _run(lib, inp, precision=1, kernel=3)
-            _assert_close(res, oracle_case(inp, "f64"), 1e-4, 1e-3, f"stream vs oracle f64 {name} rows {rows}")
+            ref64 = oracle_case(inp, "f64")
+            if name == "wide":
+                for k in _keys(ref64):
+                    a, b = np.asarray(res[k], np.float64), np.asarray(ref64[k])
+                    assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max(), (name, k)
+            else:
+                _assert_close(res, ref64, 1e-4, 1e-3, f"stream vs oracle f64 {name} rows {rows}")
             ref = _run(lib, inp, precision=1, tile=4, kernel=2)
-            _assert_close(res, ref, 1e-5, 1e-4, f"stream vs strip-split {name} rows {rows}")
+            _assert_identical(res, ref, f"stream vs strip-split {name} rows {rows}")
     finally:
         os.environ.pop("OTFWI_STREAM_ROWS", None)
 
