@@ -133,7 +133,8 @@ int otf_batch_forward(otf_batch *b, float *traces, int on_device);
 int otf_batch_forward_ring(otf_batch *b, float *traces, int on_device);
 /* Full gradient: forward, device misfit (0 = L2, 1 = Wasserstein as
  * adjoint_functions.wasserstein, 2 = Wasserstein on softplus-normalised
- * traces, 3 = adjoint_functions.wasserstein_quad), reverse phase; grad [Z*X]
+ * traces, 3 = adjoint_functions.wasserstein_quad, 4 = adjoint_functions.
+ * quad_envelope), reverse phase; grad [Z*X]
  * = mean over shots of the per-shot gradients, *misfit = sum over every
  * trace (both optional). */
 int otf_batch_gradient(otf_batch *b, int misfit_kind, float *grad, double *misfit, int on_device);
@@ -181,7 +182,9 @@ int otf_multi_sync(otf_multi *m);
 
 /* Stand-alone device misfit over n_traces traces [n_traces][T] (device
  * pointers, misfit [n_traces] FP64) with caller-owned scratch of at least
- * otf_misfit_scratch_bytes(kind, n_traces, T) bytes, on a cudaStream_t. */
+ * otf_misfit_scratch_bytes(kind, n_traces, T) bytes, on a cudaStream_t.
+ * Kind 4 (quad_envelope) creates a cuFFT plan per (n_traces, T) on its first
+ * call, which allocates: make that call outside stream capture. */
 long long otf_misfit_scratch_bytes(int kind, int n_traces, int T);
 int otf_misfit(int kind, const float *sim, const float *obs, float *adj, double *misfit,
                int n_traces, int T, void *scratch, long long scratch_bytes, void *stream);
@@ -195,7 +198,8 @@ int otf_misfit(int kind, const float *sim, const float *obs, float *adj, double 
  * above 16 MiB is rejected with an error (returns -1). The first call on a
  * device looks the array's device address up: make it before any stream
  * capture. All calls share the array: calls that may overlap on the GPU race,
- * so order them on one stream. Inputs and outputs are caller device memory. */
+ * so order them on one stream. Inputs and outputs are caller device memory.
+ * Kind 4 (quad_envelope) is refused: its FFT plans allocate. */
 int otf_misfit_noalloc(int kind, const float *sim, const float *obs, float *adj, double *misfit,
                        int n_traces, int T, void *stream);
 

@@ -98,7 +98,7 @@ def build(verbose=False, ptxas_info=False):
         if r.returncode != 0:
             raise RuntimeError(f"CPML link failed:\n{r.stdout}\n{r.stderr}")
     if jobs or _stale(LIB, objs):
-        cmd = [nvcc, "-shared", "-o", LIB] + objs + ARCH + ["-lcuda"]
+        cmd = [nvcc, "-shared", "-o", LIB] + objs + ARCH + ["-lcuda", "-lcufft"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -10,6 +10,7 @@ init_regression`` as the adjoint callback:
   wasserstein_softplus  Wasserstein on softplus-normalised traces (no
                         reference counterpart; definition in misfit.cu)
   wasserstein_quad      adjoint_functions.py:70-108
+  quad_envelope         adjoint_functions.py:14-22
 
 The arithmetic runs in the library's misfit kernels (otf_misfit); device
 memory comes from PyTorch. No CPU fallback: without a GPU these raise.
@@ -61,3 +62,7 @@ def wasserstein_softplus(sim, obs):
 
 def wasserstein_quad(sim, obs):
     return _device_misfit(MISFITS["wasserstein_quad"], sim, obs)
+
+
+def quad_envelope(sim, obs):
+    return _device_misfit(MISFITS["quad_envelope"], sim, obs)

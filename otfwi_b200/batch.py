@@ -18,7 +18,7 @@ import numpy as np
 from . import _lib
 from .cuda_interface_pml import pml_damping, ring_mask
 
-MISFITS = {"l2": 0, "wasserstein": 1, "wasserstein_softplus": 2, "wasserstein_quad": 3}
+MISFITS = {"l2": 0, "wasserstein": 1, "wasserstein_softplus": 2, "wasserstein_quad": 3, "quad_envelope": 4}
 
 
 def _declare(lib):

@@ -1193,6 +1193,8 @@ int Engine::prepare_gradient(int kind)
         OTF_CUDA(cudaMalloc(&gsum_, sizeof(float) * (size_t)cfg_.X * cfg_.Z));
         OTF_CUDA(cudaMalloc(&tot_, sizeof(double)));
     }
+    if (kind == kMisfitQuadEnvelope && envelope_prepare(n_shots_ * n_rec_, cfg_.T))
+        return -1;
     const int64_t need = misfit_scratch_per_trace(kind, cfg_.T) * n_shots_ * n_rec_;
     if (need > mscratch_bytes_) {
         drop_graphs();

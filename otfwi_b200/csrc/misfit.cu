@@ -418,6 +418,8 @@ int64_t misfit_scratch_per_trace(int kind, int T)
 {
     if (kind == kMisfitL2)
         return 0;
+    if (kind == kMisfitQuadEnvelope)
+        return envelope_scratch_per_trace(T);
     int64_t P = 1;
     while (P < T)
         P <<= 1;
@@ -444,6 +446,8 @@ int launch_misfit(int kind, const float *sim, const float *obs, float *adj, doub
     case kMisfitWassersteinSoftplus:
         k_wasserstein<2><<<n_traces, MT, 0, st>>>(sim, obs, adj, misfit, (char *)scratch, T, per);
         break;
+    case kMisfitQuadEnvelope:
+        return launch_envelope(sim, obs, adj, misfit, n_traces, T, scratch, st);
     case kMisfitWassersteinQuad:
         k_wasserstein<3><<<n_traces, MT, 0, st>>>(sim, obs, adj, misfit, (char *)scratch, T, per);
         break;
@@ -511,6 +515,8 @@ extern "C" int otf_misfit_noalloc(int kind, const float *sim, const float *obs, 
 {
     OTF_CHECK(T >= 2, 1, "otf_misfit_noalloc: T must be at least 2");
     OTF_CHECK(n_traces >= 0, 1, "otf_misfit_noalloc: negative trace count");
+    OTF_CHECK(kind != otf::kMisfitQuadEnvelope, 1,
+              "otf_misfit_noalloc: quad_envelope needs FFT plans, whose creation allocates; use otf_misfit");
     const long long need = (long long)otf::misfit_scratch_per_trace(kind, T) * n_traces;
     OTF_CHECK(need <= kNoAllocScratchBytes, 1,
               "otf_misfit_noalloc: " + std::to_string(n_traces) + " traces of " + std::to_string(T) +

@@ -9,9 +9,17 @@ enum MisfitKind : int {
     kMisfitL2 = 0,
     kMisfitWasserstein = 1,
     kMisfitWassersteinSoftplus = 2,
-    kMisfitWassersteinQuad = 3
+    kMisfitWassersteinQuad = 3,
+    kMisfitQuadEnvelope = 4
 };
-constexpr int kNumMisfits = 4;
+constexpr int kNumMisfits = 5;
+
+// quad_envelope (envelope.cu): FFT plans are created by envelope_prepare,
+// which must run outside stream capture (plan creation allocates).
+int64_t envelope_scratch_per_trace(int T);
+int envelope_prepare(int n_traces, int T);
+int launch_envelope(const float *sim, const float *obs, float *adj, double *misfit, int n, int T, void *scratch,
+                    cudaStream_t st);
 
 // Bytes of global scratch one trace needs (0 for L2).
 int64_t misfit_scratch_per_trace(int kind, int T);

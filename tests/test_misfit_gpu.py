@@ -49,6 +49,23 @@ def test_device_softplus_wasserstein_matches_oracle(lib, path):
     assert _rel_max(adj, ref) <= 1e-5
 
 
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "misfit_*.npz"))),
+                         ids=os.path.basename)
+def test_device_quad_envelope(lib, path):
+    """quad_envelope through batched cuFFT in FP64: against the FP64 oracle
+    (misfit rel 1e-9, adjoint 1e-6: FP32 output) and against the reference
+    itself (1e-5: its analytic signal of the float32 observed trace is a
+    single-precision FFT)."""
+    from otfwi_b200.batch import device_misfit
+    d = np.load(path)
+    e, ref = mo.quad_envelope(d["sim"].astype(np.float64), d["obs"])
+    m, adj = device_misfit(d["sim"], d["obs"], "quad_envelope")
+    assert abs(m.sum() - e) <= 1e-9 * abs(e)
+    assert _rel_max(adj, ref) <= 1e-6
+    assert abs(m.sum() - d["env"]) <= 1e-5 * abs(d["env"])
+    assert _rel_max(adj, d["env_adj"]) <= 1e-5
+
+
 def test_wasserstein_long_traces_and_many(lib):
     """T = 4000 traces (the FMC length), many traces in one launch."""
     from otfwi_b200.batch import device_misfit
