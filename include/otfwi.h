@@ -53,7 +53,10 @@ void init_memory_reg(float *obs, float **grad_ptr, int *rev_x, int *rev_z, int n
 void setCquad(float *cquad);
 
 /* Replaces cuda_simulate, regression_PML_single.cu:618-702: forward modelling;
- * idx_source == -1 fires every source, otherwise only source idx_source. */
+ * idx_source == -1 fires every source, otherwise only source idx_source.
+ * en_out != 0: the video frames the reference pipes into ffmpeg (8-bit grey
+ * [Z][X] per step t = 1..T-1, utils.cu:84-120) are written raw to
+ * $OTFWI_FRAMES_PATH, default output/outputPML.gray (no encoder). */
 void cuda_simulate(int en_out, int idx_source);
 
 /* Replaces cuda_grad_ext, regression_PML_single.cu:704-846: forward with ring
@@ -166,6 +169,14 @@ int otf_batch_objective(otf_batch *b, int misfit_kind, double *misfit, int on_de
 /* Source illumination illum [Z*X] = sum over shots and over every `every`-th
  * forward step of P^2 (one forward modelling). */
 int otf_batch_illumination(otf_batch *b, int every, float *illum, int on_device);
+/* Headless video (replaces the ffmpeg pipe of cuda_simulate(en_out = 1),
+ * regression_PML_single.cu:619-700 / utils.cu:84-120 writeFramePipe): one
+ * forward modelling of every shot (traces recorded as by
+ * otf_batch_forward), and at every `every`-th step t = every, 2 every, ...
+ * <= T-1 the total pressure of shot `shot` as an 8-bit grey frame [Z][X]:
+ * (P - min) * (255 / (max - min)) truncated, receivers 255. frames: host
+ * buffer of (T-1)/every * Z * X bytes. */
+int otf_batch_frames(otf_batch *b, int every, int shot, unsigned char *frames);
 /* Results of the last gradient of this batch (also after otf_multi_gradient). */
 int otf_batch_last_gradient(otf_batch *b, float *grad, double *misfit, int on_device);
 

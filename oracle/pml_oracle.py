@@ -40,8 +40,9 @@ def _load():
     lib.orc_exact_adjoint_f64.argtypes = common + [dp, dp, dp]
     lib.orc_forward_f64.argtypes = [c_int, c_int, c_int, dp, fp, fp, fp, c_int, ip, ip, fp, c_int, c_int,
                                     ip, ip, dp]
+    lib.orc_frames_f32.argtypes = common + [c_int, POINTER(ctypes.c_ubyte), fp]
     for f in (lib.orc_simulate_f32, lib.orc_simulate_f64, lib.orc_grad_f32, lib.orc_grad_f64,
-              lib.orc_num_threads, lib.orc_exact_adjoint_f64, lib.orc_forward_f64):
+              lib.orc_num_threads, lib.orc_exact_adjoint_f64, lib.orc_forward_f64, lib.orc_frames_f32):
         f.restype = c_int
     _lib = lib
     return lib
@@ -119,6 +120,23 @@ def simulate(cquad, constvec, d_x, d_z, src_x, src_z, source, rec_x, rec_z, idx_
     if rc:
         raise RuntimeError("oracle simulate failed")
     return rec
+
+
+def frames(cquad, constvec, d_x, d_z, src_x, src_z, source, rec_x, rec_z, every=1, idx_source=-1):
+    """Video frames of cuda_simulate(en_out = 1): (uint8 [(T-1)//every, Z, X],
+    the FP32 total pressure of the same steps [(T-1)//every, Z, X])."""
+    lib = _load()
+    Z, X = np.asarray(cquad).shape
+    T = np.asarray(source).reshape(len(np.atleast_1d(src_x)), -1).shape[1]
+    arrs = _prep(cquad, constvec, d_x, d_z, src_x, src_z, source, rec_x, rec_z)
+    n = (T - 1) // every
+    fr = np.zeros((n, Z, X), np.uint8)
+    pf = np.zeros((n, Z, X), np.float32)
+    rc = lib.orc_frames_f32(*_args(X, Z, T, arrs, idx_source), int(every),
+                            fr.ctypes.data_as(POINTER(ctypes.c_ubyte)), pf.ctypes.data_as(POINTER(c_float)))
+    if rc:
+        raise RuntimeError("oracle frames failed")
+    return fr, pf
 
 
 def grad(cquad, constvec, d_x, d_z, src_x, src_z, source, rec_x, rec_z, ring_x, ring_z, adj_fun,

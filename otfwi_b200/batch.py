@@ -48,6 +48,7 @@ def _declare(lib):
         "otf_batch_sync": [c_void_p],
         "otf_batch_objective": [c_void_p, c_int, c_void_p, c_int],
         "otf_batch_illumination": [c_void_p, c_int, c_void_p, c_int],
+        "otf_batch_frames": [c_void_p, c_int, c_int, c_void_p],
         "otf_misfit": [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p,
                        c_longlong, c_void_p],
     }.items():
@@ -241,6 +242,18 @@ class ShotBatch:
             out = np.zeros((self.Z, self.X), np.float32)
         p, dev = _ptr(out)
         self._ok(self._lib.otf_batch_illumination(self._h, int(every), p, dev))
+        self.sync()
+        return out
+
+    def frames(self, every=1, shot=0):
+        """Headless video of one forward modelling (the reference's
+        ``simulate(output=True)`` frames): uint8 [(T-1)//every, Z, X], the
+        total pressure of shot ``shot`` at steps every, 2 every, ... mapped
+        from the frame's [min, max] onto 0..255, receivers 255. Traces of
+        every shot are recorded as by ``forward``."""
+        n = (self.T - 1) // int(every)
+        out = np.zeros((n, self.Z, self.X), np.uint8)
+        self._ok(self._lib.otf_batch_frames(self._h, int(every), int(shot), ctypes.c_void_p(out.ctypes.data)))
         self.sync()
         return out
 

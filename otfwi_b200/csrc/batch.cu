@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <memory>
 #include <vector>
+#include <cstring>
 #include "engine.h"
 #include "misfit.h"
 #include "../../include/otfwi.h"
@@ -201,6 +202,28 @@ int otf_batch_illumination(otf_batch *b, int every, float *illum, int on_device)
         OTF_CUDA(cudaMemcpyAsync(illum, b->eng.illum_dev(), sizeof(float) * (size_t)c.X * c.Z,
                                  kind_out(on_device), b->eng.stream()));
     return 0;
+}
+
+namespace {
+struct FrameCopy {
+    unsigned char *dst;
+    size_t frame_bytes;
+};
+int copy_frames(void *ctx, const unsigned char *frames, int n)
+{
+    FrameCopy &c = *static_cast<FrameCopy *>(ctx);
+    memcpy(c.dst, frames, (size_t)n * c.frame_bytes);
+    c.dst += (size_t)n * c.frame_bytes;
+    return 0;
+}
+}  // namespace
+
+int otf_batch_frames(otf_batch *b, int every, int shot, unsigned char *frames)
+{
+    OTF_CHECK(frames != nullptr, 1, "otf_batch_frames: no output buffer");
+    const otf::EngineConfig &c = b->eng.config();
+    FrameCopy fc{frames, (size_t)c.X * c.Z};
+    return b->eng.frames(every, shot, copy_frames, &fc);
 }
 
 int otf_batch_last_gradient(otf_batch *b, float *grad, double *misfit, int on_device)

@@ -5,7 +5,10 @@
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
+#include <string>
+#include <sys/stat.h>
 #include <memory>
 #include <vector>
 #include "engine.h"
@@ -171,15 +174,57 @@ void def_python_adj(void *fn)
         g_state->python_adj = fn;
 }
 
+namespace {
+struct FrameFile {
+    FILE *fp;
+    size_t frame_bytes;
+};
+int write_frames(void *ctx, const unsigned char *frames, int n)
+{
+    FrameFile &f = *static_cast<FrameFile *>(ctx);
+    if (fwrite(frames, 1, (size_t)n * f.frame_bytes, f.fp) != (size_t)n * f.frame_bytes) {
+        otf::set_error_msg(3, "cuda_simulate: writing the video frames failed");
+        return -1;
+    }
+    return 0;
+}
+
+// en_out = 1: the frames the reference pipes into ffmpeg (8-bit grey [Z][X]
+// per step t = 1..T-1, regression_PML_single.cu:619-700) are written raw to
+// OTFWI_FRAMES_PATH, default output/outputPML.gray (the reference's
+// output/outputPML.mp4 without the encoder; `ffmpeg -f rawvideo -pix_fmt
+// gray -s XxZ -i output/outputPML.gray ...` encodes it).
+int simulate_with_frames(DropIn &s)
+{
+    const char *env = getenv("OTFWI_FRAMES_PATH");
+    std::string path = env && *env ? env : "output/outputPML.gray";
+    const size_t cut = path.find_last_of('/');
+    if (cut != std::string::npos && cut > 0)
+        mkdir(path.substr(0, cut).c_str(), 0755);  // as the reference's "mkdir -p output/..."
+    FILE *fp = fopen(path.c_str(), "wb");
+    if (!fp) {
+        otf::set_error_msg(3, "cuda_simulate: cannot open " + path);
+        return -1;
+    }
+    const otf::EngineConfig &c = s.eng.config();
+    FrameFile ff{fp, (size_t)c.X * c.Z};
+    const int rc = s.eng.frames(1, 0, write_frames, &ff);
+    if (fclose(fp) != 0 && rc == 0) {
+        otf::set_error_msg(3, "cuda_simulate: closing " + path + " failed");
+        return -1;
+    }
+    return rc;
+}
+}  // namespace
+
 void cuda_simulate(int en_out, int idx_source)
 {
-    (void)en_out;  // video output of the reference (ffmpeg pipe) is not part of this library
     if (!g_state) {
         otf::set_error_msg(2, "cuda_simulate called before init_memory_sim");
         return;
     }
     DropIn &s = *g_state;
-    if (select_shot(s, idx_source) || s.eng.forward(false) ||
+    if (select_shot(s, idx_source) || (en_out ? simulate_with_frames(s) : s.eng.forward(false)) ||
         s.eng.copy_traces(s.rec_h, 0, 1, cudaMemcpyDeviceToHost) || s.eng.sync())
         return;
 }

@@ -1060,7 +1060,7 @@ static dim3 step_grid(const EngineConfig &c, int n_shots)
 
 // Emit (into the stream, normally under capture) the forward time loop:
 // zero the fields, then one fused launch per step.
-int Engine::emit_forward(bool with_ring)
+int Engine::emit_forward(bool with_ring, StepHook hook, void *ctx)
 {
     StepParams p = base_params();
     p.q0 = qf_;
@@ -1081,6 +1081,8 @@ int Engine::emit_forward(bool with_ring)
         p.f0 = Fields{fld_[0][0][i], fld_[0][1][i], fld_[0][2][i], fld_[0][3][i],
                       fld_[0][0][o], fld_[0][1][o], fld_[0][2][o], fld_[0][3][o]};
         if (launch_forward_step(p, with_ring, grid, i, i))
+            return -1;
+        if (hook && hook(ctx, t, o))
             return -1;
     }
     return 0;

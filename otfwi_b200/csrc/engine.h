@@ -75,6 +75,13 @@ class Engine {
     int objective(int kind);
     // sum over shots and every `every`-th step of P^2 into illum_dev() [Z*X]
     int illumination(int every);
+    // Headless video of the forward modelling (frames.cu): the forward of
+    // every shot (receivers recorded as by forward(false)), and at every
+    // `every`-th step t the total pressure of shot `shot` quantised on the
+    // device to an 8-bit grey frame [Z][X] as the reference's video writer
+    // does; frames reach `sink` in order, in chunks of at most 256 MiB.
+    using FrameSink = int (*)(void *ctx, const unsigned char *frames, int n_frames);
+    int frames(int every, int shot, FrameSink sink, void *ctx);
     float *illum_dev() { return illum_; }
 
     // Differentiable path (engine_adjoint.cu): forward of every shot keeping
@@ -114,7 +121,9 @@ class Engine {
     int prepare();
     int prepare_gradient(int kind);
     int emit_gradient(int kind);
-    int emit_forward(bool with_ring);
+    // hook(ctx, t, slot) runs after the step-t launch (slot: P's output slot)
+    using StepHook = int (*)(void *ctx, int t, int slot);
+    int emit_forward(bool with_ring, StepHook hook = nullptr, void *ctx = nullptr);
     int emit_reverse();
     template <class Emit>
     int capture(cudaGraphExec_t *out, Emit emit);

@@ -151,8 +151,9 @@ def test_streaming_kernels_close_to_oracle(lib, rows):
     than two strips whose width is not a multiple of the strip, identical to
     the strip-split kernels (with dt = dx the two compute the same operations
     in the same order). On the wide grid some receivers see only numerical
-    precursors within T, so its oracle check is normalised by the largest
-    trace of the shot rather than per receiver."""
+    precursors within T and one shot's gradient is of the order of FP32
+    subnormals (its source is out of reach of every receiver), so its oracle
+    check is normalised by the largest value of each quantity over all shots."""
     import make_sim_golden
     from otfwi_b200 import scenarios
     from otfwi_b200.cuda_interface_pml import pml_damping
@@ -164,9 +165,13 @@ def test_streaming_kernels_close_to_oracle(lib, rows):
             res = _run(lib, inp, precision=1, kernel=3)
             ref64 = oracle_case(inp, "f64")
             if name == "wide":
+                fam = lambda k: k.rstrip("0123456789")
+                scale = {}
+                for k in _keys(ref64):
+                    scale[fam(k)] = max(scale.get(fam(k), 0.0), float(np.abs(ref64[k]).max()))
                 for k in _keys(ref64):
                     a, b = np.asarray(res[k], np.float64), np.asarray(ref64[k])
-                    assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max(), (name, k)
+                    assert np.abs(a - b).max() <= 1e-4 * scale[fam(k)], (name, k)
             else:
                 _assert_close(res, ref64, 1e-4, 1e-3, f"stream vs oracle f64 {name} rows {rows}")
             ref = _run(lib, inp, precision=1, tile=4, kernel=2)

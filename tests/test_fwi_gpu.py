@@ -68,3 +68,22 @@ def test_plain_descent_decreases_misfit_and_error(lib):
         assert all(x > y for x, y in zip(m, m[1:]))
     assert h.rms[-1] < h.rms[0]
     assert float(c.min()) >= prob.vmin - 1e-7 and float(c.max()) <= prob.vmax + 1e-7
+
+
+def test_lbfgsb_result_file(lib, tmp_path):
+    """The reference's L-BFGS-B driver (regression.py:82-96) end to end: a
+    few iterations over the batched GPU objective, then the closing
+    re-simulation, L2 misfit and result pickle."""
+    from otfwi_b200 import fwi, results
+    sc, prob = _problem(iters=2)
+    r, mm = fwi.lbfgsb(prob, sc.c_start, b=0, maxiter=2)
+    assert r.fun < fwi.objfun(prob, 0, sc.c_start.ravel())[0]
+    path = tmp_path / "output" / "regression_small.pickle"
+    out = results.finish(prob, r.x, r.fun, mm, str(path), b=0)
+    d = results.load(str(path))
+    sb = prob.batch(0)
+    assert d["recording"].shape == (sb.n_shots, sb.n_rec, sc.T) and d["recording"].dtype == np.float32
+    assert np.array_equal(d["model"], r.x.reshape(sc.Z, sc.X))
+    assert d["mseL2"] == results.l2(d["recording"], sb._obs_dev.cpu().numpy()) == out["mseL2"]
+    assert d["model_misfit"] == mm and len(mm) >= 1
+    assert d["vmin"] == prob.vmin and d["fun"] == r.fun
