@@ -278,7 +278,7 @@ void Engine::free_all()
     if (qr_ == qf_)
         qr_ = nullptr;  // aliased when dt == dx == 1: freed once, as qf_
     float **fl[] = {&qf_, &qr_, &dampx_, &dampz_, &dampx2_, &dampz2_, &grad_, &rec_, &ring_,
-                    &src_, &tab_src_, &adj_, &tab_adj_, &obs_, &gsum_, &illum_};
+                    &src_, &tab_src_, &adj_, &tab_adj_, &obs_, &gsum_, &illum_, &cq_stage_};
     for (float **p : fl) {
         if (*p)
             cudaFree(*p);
@@ -435,19 +435,18 @@ int Engine::set_model(const float *cquad, bool on_device)
 {
     OTF_CHECK(ready_, 2, "engine not initialised");
     const size_t n = (size_t)cfg_.X * cfg_.Z;
-    float *tmp = nullptr;
     const float *dsrc = cquad;
     if (!on_device) {
-        OTF_CUDA(cudaMallocAsync(&tmp, sizeof(float) * n, st_));
-        OTF_CUDA(cudaMemcpyAsync(tmp, cquad, sizeof(float) * n, cudaMemcpyHostToDevice, st_));
-        dsrc = tmp;
+        // a persistent staging buffer: no allocation (and no pool trim) per model update
+        if (!cq_stage_)
+            OTF_CUDA(cudaMalloc(&cq_stage_, sizeof(float) * n));
+        OTF_CUDA(cudaMemcpyAsync(cq_stage_, cquad, sizeof(float) * n, cudaMemcpyHostToDevice, st_));
+        dsrc = cq_stage_;
     }
     const int bs = 256;
     const int nb = (int)((L_.slot + bs - 1) / bs);
     k_prep_q<<<nb, bs, 0, st_>>>(dsrc, qf_, two_q_ ? qr_ : nullptr, L_, cfg_.dx, cfg_.dt);
     OTF_CUDA(cudaGetLastError());
-    if (tmp)
-        OTF_CUDA(cudaFreeAsync(tmp, st_));
     return 0;
 }
 

@@ -146,6 +146,7 @@ class Engine {
     cudaStream_t st_ = nullptr;
     // device buffers
     float *qf_ = nullptr, *qr_ = nullptr;                            // padded P coefficients
+    float *cq_stage_ = nullptr;                                      // [Z*X] staging of a host model
     float *dampx_ = nullptr, *dampz_ = nullptr;                      // separable multipliers
     float *dampx2_ = nullptr, *dampz2_ = nullptr;                    // general multipliers
     float *fld_[2][4][2] = {};  // [set][Px,Pz,Ax,Az][slot], each [max_shots][slot floats]

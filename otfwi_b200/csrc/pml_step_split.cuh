@@ -63,7 +63,9 @@ __device__ __forceinline__ void dstag_n(const float *w, float *out)
     }
 }
 
-// 9-point second derivative at N consecutive cells from N+8 values.
+// 9-point second-derivative tap sums (the weights times 5040) at N
+// consecutive cells from N+8 values; lap_combine turns the x and z sums into
+// the Laplacian with one rounded scaling instead of a division per axis.
 template <int N>
 __device__ __forceinline__ void lap_n(const float *w, float *out)
 {
@@ -79,8 +81,14 @@ __device__ __forceinline__ void lap_n(const float *w, float *out)
         s = __fmaf_rn(-1008.0f, m[-2], s);
         s = __fmaf_rn(128.0f, m[-3], s);
         s = __fmaf_rn(-9.0f, m[-4], s);
-        out[j] = __fdiv_rn(s, 5040.0f);
+        out[j] = s;
     }
+}
+
+__device__ __forceinline__ float lap_combine(float sx, float sz)
+{
+    constexpr float inv = (float)(1.0 / 5040.0);
+    return __fmul_rn(__fadd_rn(sx, sz), inv);
 }
 
 enum Inject : int { kInjNone = 0, kInjSources = 1, kInjReceivers = 2 };
@@ -263,7 +271,7 @@ __device__ __forceinline__ void a_split(const StepParams &p, const float *sAx, c
                     lap_n<BH>(v[j], l);
 #pragma unroll
                     for (int i = 0; i < BH; i++)
-                        lap[kb][4 * i + j] = __fadd_rn(lap[kb][4 * i + j], l[i]);
+                        lap[kb][4 * i + j] = lap_combine(lap[kb][4 * i + j], l[i]);
                 }
             }
         }
@@ -507,8 +515,10 @@ __global__ void __launch_bounds__(NTH, MINB) k_reverse_split(const __grid_consta
                 p_split<TX, TZ, BH, NTH, false, true, kInjNone>(p, sAx, sAz, sPo, nullptr, sq, sP,
                                                                 nullptr, x0, z0, shot, tile);
             __syncthreads();
-            ring_overwrite1(p, sP, shot, tile, NTH);
-            __syncthreads();
+            if (p.ringe_ptr[tile + 1] > p.ringe_ptr[tile]) {  // uniform per item
+                ring_overwrite1(p, sP, shot, tile, NTH);
+                __syncthreads();
+            }
             store_p1<TX, TZ>(p, sP, p.f0.px_out + so, x0, z0, NTH);
             if (edge)
                 a_split<TX, TZ, BH, NTH, true, true, true>(p, sAx, sAz, sP, p.f0.ax_out + so,

@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(SC, MINB) k_reverse_stream(const __grid_consta
                 float lx, lz;
                 lap_n<1>(rr + i - 4, &lx);
                 lap_n<1>(pwr, &lz);
-                p.grad[o] = __fmaf_rn(pwa[3], __fadd_rn(lx, lz), gold);
+                p.grad[o] = __fmaf_rn(pwa[3], lap_combine(lx, lz), gold);
 #pragma unroll
                 for (int j = 0; j < 8; j++)
                     wp[j] = ra[i - 3 + j];

@@ -65,7 +65,7 @@ def test_batch_frames_of_one_shot(lib, precision):
     sc = scenarios.small(X=128, Z=96, T=300, n_src=3, n_rec=10, seed=21, f0=0.035)
     inp = make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))
     b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, precision=precision)
-    b.set_model(sc.c_true)
+    b.set_model(inp["c_true"])  # the FP32 model the oracle squares
     got = b.frames(every=5, shot=1)
     ref = _oracle_frames(inp, 5, idx_source=1)
     assert got.shape == ref.shape
