@@ -133,10 +133,14 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per cell of one reverse-step launch from the committed ncu
-    summary (profiles/reverse_step_fmc.md, line 'dram_bytes_per_cell: N')."""
-    p = os.path.join(ROOT, "profiles", "reverse_step_fmc.md")
+def profile_traffic(kernel):
+    """DRAM bytes per cell of one reverse step from the committed ncu summary
+    of the kernel variant in use (line 'dram_bytes_per_cell: N'):
+    profiles/reverse_step_fmc.md for the fused strip-split step (one
+    launch), profiles/reverse_step_unfused_fmc.md for the unfused one (its
+    three launches summed)."""
+    name = "reverse_step_unfused_fmc.md" if kernel == 4 else "reverse_step_fmc.md"
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -256,8 +260,13 @@ def run_ours(args):
     per_launch_cells = sc.X * sc.Z * sc.n_src
     ach_rev = BYTES_REV * per_launch_cells / (ms_rev / 1e3) / 1e9
     ach_fwd = BYTES_FWD * per_launch_cells / (ms_fwd / 1e3) / 1e9
-    tr = profile_traffic()
-    roof = {"kernel": "k_reverse_step (adjoint + reconstruction + imaging condition, all shots)",
+    tr = profile_traffic(args.kernel)
+    if args.kernel == 4:
+        rev_name = ("reverse step (k_unfused_p_rev + k_unfused_ring + k_unfused_a_rev: adjoint + "
+                    "reconstruction + imaging condition, all shots; 88 B/cell moved)")
+    else:
+        rev_name = "k_reverse_split (adjoint + reconstruction + imaging condition, all shots)"
+    roof = {"kernel": rev_name,
             "bound": "hbm", "achieved": round(ach_rev, 1), "peak": peak, "unit": "GB/s",
             "frac": round(ach_rev / peak, 4), "peak_kind": peak_kind,
             "traffic": (tr * per_launch_cells if tr else None),

@@ -9,8 +9,9 @@ so the search runs once per configuration.
 
 Candidates: tile shapes 0 (56x56), 1 (120x24), 4 (56x24) with the persistent
 TMA kernels (variant 1) and, for the fast numerics, the strip-split kernels
-(variant 2); shapes 2 (120x56) and 3 (248x24) with the one-tile-per-CTA
-kernels (variant 0).
+(variant 2) and the unfused streaming half-steps (variant 4, no tiles);
+shapes 2 (120x56) and 3 (248x24) with the one-tile-per-CTA kernels
+(variant 0).
 """
 import json
 import os
@@ -24,7 +25,7 @@ TILES = {0: (56, 56), 1: (120, 24), 2: (120, 56), 3: (248, 24), 4: (56, 24)}
 def candidates(precision):
     c = [(1, 0), (1, 1), (1, 4), (0, 2), (0, 3)]
     if precision == 1:
-        c = [(2, 0), (2, 1), (2, 4)] + c
+        c = [(4, 4), (2, 0), (2, 1), (2, 4)] + c
     return c
 
 
@@ -34,7 +35,8 @@ def cache_path():
 
 
 def _key(X, Z, shots, n_rec, precision, gpu):
-    return f"{gpu}|{X}x{Z}|shots{shots}|rx{n_rec}|prec{precision}"
+    cands = ",".join(f"{k}/{t}" for k, t in candidates(precision))
+    return f"{gpu}|{X}x{Z}|shots{shots}|rx{n_rec}|prec{precision}|{cands}"
 
 
 def _load():

@@ -185,7 +185,8 @@ class ShotBatch:
     def set_kernel(self, variant):
         """-1: automatic; 0: one tile per CTA per step; 1: persistent
         TMA-pipelined CTAs; 2: persistent strip-split kernels (fast numerics);
-        3: z-streaming strips (fast numerics)."""
+        3: z-streaming strips (fast numerics); 4: unfused streaming
+        half-steps (fast numerics)."""
         self._ok(self._lib.otf_batch_set_kernel(self._h, variant))
 
     def set_stream_rows(self, rows):

@@ -8,6 +8,7 @@
 #include <cudaTypedefs.h>
 #include "engine.h"
 #include "misfit.h"
+#include "pml_step_unfused.cuh"
 
 namespace otf {
 
@@ -768,6 +769,47 @@ int Engine::build_tables()
         h.insert(h.end(), id.begin(), id.end());
         h.push_back(0);
     }
+    // unfused kernels: distinct injection cells (padded offset) with their
+    // source / receiver indices in increasing order (CSR); padded offsets of
+    // receivers and ring cells
+    const int NCB = (X + kUCols - 1) / kUCols, NSEG = (Z + kURows - 1) / kURows;
+    size_t o_usrc = 0, o_urcv = 0;
+    int n_ucells[2] = {0, 0};
+    for (int pass = 0; pass < 2; pass++) {
+        std::vector<std::pair<int, int>> pts;  // (offset, index)
+        if (pass == 0)
+            for (int k = 0; k < n_src_; k++)
+                pts.push_back({(int)L_.at(src_x_[k], src_z_[k]), k});
+        else
+            for (int n = 0; n < n_rec_; n++)
+                if (interior(rec_x_[n], rec_z_[n], X, Z))
+                    pts.push_back({(int)L_.at(rec_x_[n], rec_z_[n]), n});
+        std::stable_sort(pts.begin(), pts.end());
+        std::vector<int> ptr(1, 0), off, id;
+        for (size_t e = 0; e < pts.size(); e++) {
+            if (e == 0 || pts[e].first != pts[e - 1].first) {
+                off.push_back(pts[e].first);
+                if (e > 0)
+                    ptr.push_back((int)e);
+            }
+            id.push_back(pts[e].second);
+        }
+        if (!pts.empty())
+            ptr.push_back((int)pts.size());
+        n_ucells[pass] = (int)off.size();
+        (pass ? o_urcv : o_usrc) = h.size();
+        h.insert(h.end(), ptr.begin(), ptr.end());
+        h.insert(h.end(), off.begin(), off.end());
+        h.push_back(0);
+        h.insert(h.end(), id.begin(), id.end());
+        h.push_back(0);
+    }
+    const size_t o_uoff = h.size();
+    for (int n = 0; n < n_rec_; n++)
+        h.push_back((int)L_.at(rec_x_[n], rec_z_[n]));
+    for (int n = 0; n < n_ring_; n++)
+        h.push_back((int)L_.at(ring_x_[n], ring_z_[n]));
+    h.push_back(0);
     const size_t o_redge = h.size();
     for (int rr = 0; rr < NR; rr++) {
         const int z = rr - PAD;
@@ -835,6 +877,19 @@ int Engine::build_tables()
     stb_.row_edge = d + o_redge;
     stb_.strip_edge = d + o_sedge;
     n_strips_ = NS;
+    // CSR blocks: ptr [cells + 1] (just [0] when empty), off [cells] + 1, id + 1
+    utb_.src_ptr = d + o_usrc;
+    utb_.src_off = utb_.src_ptr + n_ucells[0] + 1;
+    utb_.src_id = utb_.src_off + n_ucells[0] + 1;
+    utb_.rcv_ptr = d + o_urcv;
+    utb_.rcv_off = utb_.rcv_ptr + n_ucells[1] + 1;
+    utb_.rcv_id = utb_.rcv_off + n_ucells[1] + 1;
+    utb_.n_src_cells = n_ucells[0];
+    utb_.n_rcv_cells = n_ucells[1];
+    utb_.rec_off = d + o_uoff;
+    utb_.ring_off = utb_.rec_off + n_rec_;
+    utb_.ncb = NCB;
+    utb_.nseg = NSEG;
     tables_dirty_ = false;
     drop_graphs();
     return 0;
@@ -901,7 +956,49 @@ int Engine::variant_in_use() const
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
     if (variant_ == 3 && cfg_.precision == kFast && sep_ && cfg_.X % 4 == 0)
         return 3;
-    return resolve_variant(k, variant_ == 3 ? 2 : variant_, cfg_.precision);
+    if (variant_ == 4 && cfg_.precision == kFast && sep_)
+        return 4;
+    return resolve_variant(k, variant_ >= 3 ? 2 : variant_, cfg_.precision);
+}
+
+// Unfused half-step launches (pml_step_unfused.cuh): forward P then A (with
+// the receiver / ring recording CTAs); reverse P of both sets, the ring
+// overwrite, then A of both sets with the imaging condition.
+int Engine::launch_unfused(const StepParams &p, int kind)
+{
+    UnfusedParams U;
+    U.p = p;
+    U.ncb = utb_.ncb;
+    U.nseg = utb_.nseg;
+    U.src_ptr = utb_.src_ptr;
+    U.src_off = utb_.src_off;
+    U.src_id = utb_.src_id;
+    U.n_src_cells = utb_.n_src_cells;
+    U.rcv_ptr = utb_.rcv_ptr;
+    U.rcv_off = utb_.rcv_off;
+    U.rcv_id = utb_.rcv_id;
+    U.n_rcv_cells = utb_.n_rcv_cells;
+    U.rec_off = utb_.rec_off;
+    U.ring_off = utb_.ring_off;
+    U.record_ring = kind == 1;
+    const dim3 grid(U.ncb, U.nseg, n_shots_);
+    if (kind < 2) {
+        k_unfused_p_fwd<<<grid, kUThreads, 0, st_>>>(U);
+        if (U.n_src_cells > 0)
+            k_unfused_points<false><<<dim3((U.n_src_cells + 127) / 128, n_shots_), 128, 0, st_>>>(U);
+        const int extra = n_rec_ + (kind == 1 ? n_ring_ : 0);
+        const int per_row = U.ncb * kUThreads * kUTailPer;
+        const int tail = (extra + per_row - 1) / per_row;
+        k_unfused_a_fwd<<<dim3(U.ncb, U.nseg + tail, n_shots_), kUThreads, 0, st_>>>(U);
+    } else {
+        k_unfused_p_rev<<<dim3(U.ncb, U.nseg, 2 * n_shots_), kUThreads, 0, st_>>>(U, n_shots_);
+        const int np = n_ring_ + U.n_rcv_cells;
+        if (np > 0)
+            k_unfused_points<true><<<dim3((np + 127) / 128, n_shots_), 128, 0, st_>>>(U);
+        k_unfused_a_rev<<<grid, kUThreads, 0, st_>>>(U);
+    }
+    OTF_CUDA(cudaGetLastError());
+    return 0;
 }
 
 // Persistent grid of a z-streaming kernel: resident CTAs per SM x SMs.
@@ -944,6 +1041,8 @@ int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, 
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
     const int v = variant_in_use();
+    if (v == 4)
+        return launch_unfused(p, with_ring ? 1 : 0);
     if (v == 3)
         return launch_stream(p, with_ring ? 1 : 0);
     if (v >= 1) {
@@ -977,6 +1076,8 @@ int Engine::launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
     const int v = variant_in_use();
+    if (v == 4)
+        return launch_unfused(p, 2);
     if (v == 3)
         return launch_stream(p, 2);
     if (v >= 1) {
@@ -1042,7 +1143,7 @@ int Engine::set_stream_rows(int rows)
 
 int Engine::set_variant(int variant)
 {
-    OTF_CHECK(variant >= -1 && variant <= 3, 1, "unknown kernel variant");
+    OTF_CHECK(variant >= -1 && variant <= 4, 1, "unknown kernel variant");
     if (variant != variant_) {
         variant_ = variant;
         drop_graphs();

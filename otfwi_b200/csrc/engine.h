@@ -106,7 +106,8 @@ class Engine {
     int set_tile(int tile);
     // -1 automatic (default); 0 one tile per CTA; 1 persistent TMA-pipelined;
     // 2 persistent strip-split (fast numerics); 3 z-streaming strips (fast
-    // numerics, separable damping, X a multiple of 4). Falls back where not
+    // numerics, separable damping, X a multiple of 4); 4 unfused streaming
+    // half-steps (fast numerics, separable damping). Falls back where not
     // compiled or not applicable.
     int set_variant(int variant);
     // rows per segment of the z-streaming kernels (>= 8)
@@ -130,6 +131,7 @@ class Engine {
     int launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, int pin, int ain);
     int launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain, int in1);
     int launch_stream(const StepParams &p, int kind);  // 0 forward, 1 forward + ring, 2 reverse
+    int launch_unfused(const StepParams &p, int kind);  // 0 forward, 1 forward + ring, 2 reverse
     void drop_graphs();
     StepParams base_params() const;
     void free_all();
@@ -196,6 +198,11 @@ class Engine {
     int variant_ = -1;
     // z-streaming kernel tables (built with the other tables)
     StreamTabs stb_{};
+    // unfused kernels: per-CTA injection lists, receiver and ring offsets
+    struct {
+        const int *src_ptr, *src_off, *src_id, *rcv_ptr, *rcv_off, *rcv_id, *rec_off, *ring_off;
+        int n_src_cells, n_rcv_cells, ncb, nseg;
+    } utb_{};
     int n_strips_ = 0, seg_h_ = 64;
     int *derr_ = nullptr;         // device error flag of the bounded waits
     TmaParams *tmap_ = nullptr;   // tensor maps of every field, slot and coefficient

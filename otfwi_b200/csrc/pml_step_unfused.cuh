@@ -2,106 +2,77 @@
 //
 // The fused kernels (pml_step_split.cuh, pml_step_stream.cuh) compute P(t)
 // and A(t) of a tile in one pass, recomputing P on a 4-cell halo and
-// synchronising the CTA between the two half-steps. Here each half-step is
-// its own launch over the whole batch and every cell is computed once:
+// synchronising the CTA between the two half-steps; measured, they run
+// latency- and barrier-bound near half of the HBM bandwidth. Here each
+// half-step is its own launch over the whole batch, every cell is computed
+// once, and nothing waits on anything but its own loads:
 //
-//   forward step:  P kernel  P(t), Q(t) from P, Q, Ax, Az (t-1), sources
+//   forward step:  P kernel  P(t), Q(t) from P, Q, Ax, Az (t-1)
+//                  points    the shot's sources injected
 //                  A kernel  Ax, Az (t) from P(t); extra CTAs record the
 //                            receivers and the boundary ring
 //   reverse step:  P kernel  both field sets: reconstruction (undamped,
-//                            reverted) and adjoint (damped, receivers)
-//                  ring      P_rec(t) = ring(T-1-t) on the ring cells
+//                            reverted) and adjoint (damped)
+//                  points    P_rec(t) = ring(T-1-t) on the ring cells, the
+//                            adjoint sources injected at the receivers
 //                  A kernel  both A updates, the 9-point Laplacian of
 //                            P_rec(t) and grad += P_adj(t) * lap
 //
-// A thread owns one column of a 128-column block and marches down R rows:
-// z-derivatives come from a sliding register window of the column, the
-// x-derivatives from eight neighbouring columns read through L1. No shared
-// memory, no block barrier, about 32 registers: the SMs hold up to 16 CTAs
-// and the loads of many rows are in flight. The cell arithmetic is that of
-// the strip-split kernels (same pair-form staggered sums, same update and
-// injection order), with the damped A update used exactly on damped cells.
-// This moves 40 bytes per forward cell-step and 92 per reverse cell-step
-// instead of 28 and 64, and trades them for full-rate streaming.
+// A thread owns 4 adjacent columns (16-byte loads and stores) of a
+// 128-column block and marches down kURows rows: z-derivatives come from a
+// sliding register window per column, x-derivatives from three 16-byte row
+// loads (columns x-4 .. x+7) that L1 shares between neighbouring threads.
+// One warp per CTA, no shared memory, no barrier. Bytes per cell: 40 for a
+// forward step (P kernel 20 + Q on damped cells, A kernel 20), 88 for a
+// reverse step, against 28 and 64 for the fused kernels, at 80-90% of the
+// bandwidth instead of under 50%.
+//
+// The cell arithmetic is that of the strip-split kernels: the same pair-form
+// staggered sums, P and Q updates, injection (after the cell's update, in
+// source order) and Laplacian; the damped
+// A update fma(A, dm, r*D) is used exactly on damped cells (the strip-split
+// kernels use it on every cell of a tile that holds a damped cell, so the
+// two agree bit for bit when dt/dx = 1 and within rounding otherwise).
 #pragma once
 #include "pml_step.cuh"
 #include "pml_step_split.cuh"
 
 namespace otf {
 
-constexpr int kUCols = 128;  // columns (threads) per CTA
+constexpr int kUThreads = 32;             // threads per CTA
+constexpr int kUCols = 4 * kUThreads;     // columns per CTA
+constexpr int kURows = 8;                 // rows marched by a thread
+constexpr int kUTailPer = 8;              // receiver / ring cells recorded per thread
 
 struct UnfusedParams {
     StepParams p;
     int ncb, nseg;  // column blocks, row segments per shot
-    // injection points per stencil CTA (cb + ncb * seg), in source / receiver
-    // order: local column | local row << 8, and the source / receiver index
-    const int *src_ptr, *src_pos, *src_id;
-    const int *rcv_ptr, *rcv_pos, *rcv_id;
-    // padded offsets of the receivers and of the ring cells (ring order)
-    const int64_t *rec_off, *ring_off;
+    // injection cells (CSR): padded offset of each distinct cell holding a
+    // source / an injectable receiver, and its source / receiver indices in
+    // increasing order
+    const int *src_ptr, *src_off, *src_id;
+    int n_src_cells;
+    const int *rcv_ptr, *rcv_off, *rcv_id;
+    int n_rcv_cells;
+    // padded offsets (within a shot) of the receivers and of the ring cells
+    // (ring id = the caller's ring index)
+    const int *rec_off, *ring_off;
     int record_ring;  // forward: also record the boundary ring
 };
 
-__device__ __forceinline__ float ustag(const float *u)
+__device__ __forceinline__ float4 uld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ float4 uld4c(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ void ust4(float *p, const float *v)
 {
-    float o;
-    dstag_n<1>(u, &o);
-    return o;
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// Injection points of this thread's column within the CTA's segment: the
-// first two are kept in registers; more (never seen in practice) switch the
-// thread to a scan of the CTA's list per row.
-struct ColumnPoints {
-    int r0 = -1, id0 = 0, r1 = -1, id1 = 0;
-    int e_begin = 0, e_end = 0;
-    bool scan = false;
-};
-
-__device__ __forceinline__ ColumnPoints column_points(const int *ptr, const int *pos, const int *id, int cta)
-{
-    ColumnPoints c;
-    c.e_begin = ptr[cta];
-    c.e_end = ptr[cta + 1];
-    int n = 0;
-    for (int e = c.e_begin; e < c.e_end; e++) {
-        const int v = pos[e];
-        if ((v & 0xff) != (int)threadIdx.x)
-            continue;
-        if (n == 0) {
-            c.r0 = v >> 8;
-            c.id0 = id[e];
-        } else if (n == 1) {
-            c.r1 = v >> 8;
-            c.id1 = id[e];
-        }
-        n++;
-    }
-    c.scan = n > 2;
-    return c;
-}
-
-// P += I (both split components get I/2), Q += I/2 on strip cells
-template <bool SOURCES>
-__device__ __forceinline__ void inject_one(const StepParams &p, int shot, int id, bool strip, float &pn, float &qn)
-{
-    const int row = SOURCES ? p.fire_row[shot * p.n_src + id] : shot * p.n_sen + id;
-    if (row < 0)
-        return;
-    const float I = p.inj_tab[(int64_t)row * p.T + p.t];
-    pn = __fadd_rn(pn, I);
-    if (strip)
-        qn = __fadd_rn(qn, __fmul_rn(I, 0.5f));
-}
-
-// One column segment of a P half-step. REVERT: time-reversed reconstruction
-// (undamped, no Q, no injection); otherwise damped with the strip component
-// Q and point injection (SOURCES: the shot's firing sources, else the
-// adjoint sources at the receivers).
-template <int R, bool REVERT, bool SOURCES>
-__device__ __forceinline__ void p_column(const UnfusedParams &U, const Fields &f, const float *__restrict__ q,
-                                         int shot, int x, int z0, int cta)
+// One 4-column segment of a P half-step. REVERT: time-reversed
+// reconstruction (undamped, no Q); otherwise damped with the strip
+// component Q. Point injection follows in k_unfused_points.
+template <bool REVERT>
+__device__ __forceinline__ void p_segment(const UnfusedParams &U, const Fields &f, const float *__restrict__ q,
+                                          int shot, int x, int z0)
 {
     const StepParams &p = U.p;
     const int64_t so = p.shot_stride * shot;
@@ -111,102 +82,108 @@ __device__ __forceinline__ void p_column(const UnfusedParams &U, const Fields &f
     const float *__restrict__ QI = f.pz_in + so;
     float *__restrict__ PO = f.px_out + so;
     float *__restrict__ QO = f.pz_out + so;
-    const int64_t col = x + PAD;
-    const int64_t pitch = p.pitch;
-    ColumnPoints pts;
-    if (!REVERT)
-        pts = SOURCES ? column_points(U.src_ptr, U.src_pos, U.src_id, cta)
-                      : column_points(U.rcv_ptr, U.rcv_pos, U.rcv_id, cta);
-    const float dmx = REVERT ? 1.f : __ldg(p.dampx + col);
-    const bool xin = x >= 4 && x < p.X - 4;
-    float w[8];
+    const int64_t col = x + PAD, pitch = p.pitch;
+    float w[4][8];
 #pragma unroll
-    for (int k = 0; k < 7; k++)
-        w[k] = __ldg(AZ + (int64_t)(z0 - 4 + k + PAD) * pitch + col);
-    const int nz = min(R, p.Z - z0);
-#pragma unroll 4
+    for (int k = 0; k < 7; k++) {
+        const float4 v = uld4(AZ + (int64_t)(z0 - 4 + k + PAD) * pitch + col);
+        w[0][k] = v.x;
+        w[1][k] = v.y;
+        w[2][k] = v.z;
+        w[3][k] = v.w;
+    }
+    const int nz = min(kURows, p.Z - z0);
+#pragma unroll 2
     for (int r = 0; r < nz; r++) {
         const int z = z0 + r;
         const int64_t o = (int64_t)(z + PAD) * pitch + col;
-        w[7] = __ldg(AZ + o + 3 * pitch);
-        float u[8];
+        {
+            const float4 v = uld4(AZ + o + 3 * pitch);
+            w[0][7] = v.x;
+            w[1][7] = v.y;
+            w[2][7] = v.z;
+            w[3][7] = v.w;
+        }
+        float u[12], po[4], qv[4];
+        f4a(uld4(AX + o - 4), u);
+        f4a(uld4(AX + o), u + 4);
+        f4a(uld4(AX + o + 4), u + 8);
+        f4a(uld4(PI + o), po);
+        f4a(uld4(q + o), qv);
+        float dmx[4] = {1.f, 1.f, 1.f, 1.f};
+        if (!REVERT)
+            f4a(uld4(p.dampx + col), dmx);  // L1-resident, reloaded per row
+        const float dmz = REVERT ? 1.f : __ldg(p.dampz + z + PAD);
+        const bool damp = !REVERT && (dmx[0] != 1.f || dmx[1] != 1.f || dmx[2] != 1.f || dmx[3] != 1.f ||
+                                      dmz != 1.f);
+        float qo[4] = {0.f, 0.f, 0.f, 0.f};
+        if (damp)
+            f4a(uld4(QI + o), qo);
+        const bool zin = z >= 4 && z < p.Z - 4;
+        float pn[4], qn[4];
 #pragma unroll
-        for (int k = 0; k < 8; k++)
-            u[k] = __ldg(AX + o - 4 + k);
-        const float dAx = ustag(u), dAz = ustag(w);
-        const float po = __ldg(PI + o), qv = __ldg(q + o);
-        const float s = __fadd_rn(dAx, dAz);
-        float pn, qn = 0.f;
-        bool strip = false;
-        if (REVERT) {
-            pn = __fmaf_rn(-qv, s, po);
-        } else {
-            const float dmz = __ldg(p.dampz + z + PAD);
-            if (dmx != 1.f || dmz != 1.f) {
-                strip = true;
-                const float qo = __ldg(QI + o);
-                const float q1 = __fmaf_rn(qo, dmx, __fmul_rn(qv, dAx));
-                const float z1 = __fmaf_rn(__fsub_rn(po, qo), dmz, __fmul_rn(qv, dAz));
-                qn = q1;
-                pn = __fadd_rn(q1, z1);
+        for (int j = 0; j < 4; j++) {
+            float dAx, dAz;
+            dstag_n<1>(u + j, &dAx);
+            dstag_n<1>(w[j], &dAz);
+            const float s = __fadd_rn(dAx, dAz);
+            qn[j] = 0.f;
+            if (REVERT) {
+                pn[j] = __fmaf_rn(-qv[j], s, po[j]);
+            } else if (dmx[j] != 1.f || dmz != 1.f) {
+                const float q1 = __fmaf_rn(qo[j], dmx[j], __fmul_rn(qv[j], dAx));
+                const float z1 = __fmaf_rn(__fsub_rn(po[j], qo[j]), dmz, __fmul_rn(qv[j], dAz));
+                qn[j] = q1;
+                pn[j] = __fadd_rn(q1, z1);
             } else {
-                pn = __fmaf_rn(qv, s, po);
+                pn[j] = __fmaf_rn(qv[j], s, po[j]);
+            }
+            if (x + j < 4 || x + j >= p.X - 4 || !zin) {
+                pn[j] = 0.f;
+                qn[j] = 0.f;
             }
         }
-        if (!xin || z < 4 || z >= p.Z - 4) {
-            pn = 0.f;
-            qn = 0.f;
-        }
-        if (!REVERT) {
-            if (pts.scan) {
-                for (int e = pts.e_begin; e < pts.e_end; e++) {
-                    const int v = SOURCES ? U.src_pos[e] : U.rcv_pos[e];
-                    if ((v & 0xff) == (int)threadIdx.x && (v >> 8) == r)
-                        inject_one<SOURCES>(p, shot, SOURCES ? U.src_id[e] : U.rcv_id[e], strip, pn, qn);
-                }
-            } else {
-                if (pts.r0 == r)
-                    inject_one<SOURCES>(p, shot, pts.id0, strip, pn, qn);
-                if (pts.r1 == r)
-                    inject_one<SOURCES>(p, shot, pts.id1, strip, pn, qn);
-            }
-        }
-        PO[o] = pn;
-        if (strip)
-            QO[o] = qn;
+        ust4(PO + o, pn);
+        if (damp)
+            ust4(QO + o, qn);
 #pragma unroll
-        for (int k = 0; k < 7; k++)
-            w[k] = w[k + 1];
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int k = 0; k < 7; k++)
+                w[j][k] = w[j][k + 1];
     }
 }
 
+// Resident CTAs each kernel is compiled for (a register cap), from
+// measurements: 24 (80 registers) for the P kernels, 28 (72) for the forward
+// A kernel; the reverse A kernel needs its 128 registers.
+constexpr int kUPMinBlocks = 24;
+constexpr int kUAMinBlocks = 28;
+
 // Forward P half-step: grid (ncb, nseg, n_shots).
-template <int R>
-__global__ void __launch_bounds__(kUCols) k_unfused_p_fwd(const __grid_constant__ UnfusedParams U)
+__global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const __grid_constant__ UnfusedParams U)
 {
-    const int x = blockIdx.x * kUCols + threadIdx.x;
+    const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= U.p.X)
         return;
-    p_column<R, false, true>(U, U.p.f0, U.p.q0, blockIdx.z, x, blockIdx.y * R, blockIdx.x + U.ncb * blockIdx.y);
+    p_segment<false>(U, U.p.f0, U.p.q0, blockIdx.z, x, blockIdx.y * kURows);
 }
 
 // Reverse P half-steps of both sets: grid (ncb, nseg, 2 * n_shots); z <
 // n_shots: reconstruction (set 0, q0), else adjoint (set 1, q1).
-template <int R>
-__global__ void __launch_bounds__(kUCols) k_unfused_p_rev(const __grid_constant__ UnfusedParams U, int n_shots)
+__global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_rev(const __grid_constant__ UnfusedParams U, int n_shots)
 {
-    const int x = blockIdx.x * kUCols + threadIdx.x;
+    const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= U.p.X)
         return;
-    const int cta = blockIdx.x + U.ncb * blockIdx.y;
     if ((int)blockIdx.z < n_shots)
-        p_column<R, true, false>(U, U.p.f0, U.p.q0, blockIdx.z, x, blockIdx.y * R, cta);
+        p_segment<true>(U, U.p.f0, U.p.q0, blockIdx.z, x, blockIdx.y * kURows);
     else
-        p_column<R, false, false>(U, U.p.f1, U.p.q1, blockIdx.z - n_shots, x, blockIdx.y * R, cta);
+        p_segment<false>(U, U.p.f1, U.p.q1, blockIdx.z - n_shots, x, blockIdx.y * kURows);
 }
 
 // A update of one cell from the staggered derivatives of P(t): reverted,
-// undamped (single rounding) or damped.
+// damped, or undamped with a single rounding.
 __device__ __forceinline__ void a_update(const StepParams &p, bool revert, float dmx, float dmz, float dx, float dz,
                                          float ax, float az, bool in, float &nx, float &nz)
 {
@@ -226,135 +203,243 @@ __device__ __forceinline__ void a_update(const StepParams &p, bool revert, float
     }
 }
 
-// Forward A half-step: grid (ncb, nseg + n_tail, n_shots); rows of CTAs
-// past nseg record the receivers (and the ring) of their shot.
-template <int R>
-__global__ void __launch_bounds__(kUCols) k_unfused_a_fwd(const __grid_constant__ UnfusedParams U)
+// Forward A half-step: grid (ncb, n_tail + nseg, n_shots); the first n_tail
+// rows of CTAs record the receivers (and the ring) of their shot: first, so
+// that these latency-bound CTAs run beside the stencil CTAs, not after them.
+__global__ void __launch_bounds__(kUThreads, kUAMinBlocks) k_unfused_a_fwd(const __grid_constant__ UnfusedParams U)
 {
     const StepParams &p = U.p;
     const int shot = blockIdx.z;
     const int64_t so = p.shot_stride * shot;
     const float *__restrict__ P = p.f0.px_out + so;
-    if ((int)blockIdx.y >= U.nseg) {
-        const int i = ((blockIdx.y - U.nseg) * U.ncb + blockIdx.x) * kUCols + threadIdx.x;
-        if (i < p.n_sen) {
-            p.rec[((int64_t)shot * p.n_sen + i) * p.T + p.t] = P[U.rec_off[i]];
-        } else if (U.record_ring && i - p.n_sen < p.n_ring) {
-            const int k = i - p.n_sen;
-            p.ring[((int64_t)shot * p.T + p.t) * p.n_ring + k] = P[U.ring_off[k]];
+    const int n_tail = gridDim.y - U.nseg;
+    if ((int)blockIdx.y < n_tail) {
+        // recording CTAs: each thread records up to kUTailPer cells, strided
+        const int n = p.n_sen + (U.record_ring ? p.n_ring : 0);
+        const int stride = n_tail * U.ncb * kUThreads;
+        for (int i = (blockIdx.y * U.ncb + blockIdx.x) * kUThreads + threadIdx.x; i < n; i += stride) {
+            if (i < p.n_sen) {
+                p.rec[((int64_t)shot * p.n_sen + i) * p.T + p.t] = P[U.rec_off[i]];
+            } else {
+                const int k = i - p.n_sen;
+                p.ring[((int64_t)shot * p.T + p.t) * p.n_ring + k] = P[U.ring_off[k]];
+            }
         }
         return;
     }
-    const int x = blockIdx.x * kUCols + threadIdx.x;
+    const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= p.X)
         return;
-    const int z0 = blockIdx.y * R;
+    const int z0 = (blockIdx.y - n_tail) * kURows;
     const float *__restrict__ AXI = p.f0.ax_in + so;
     const float *__restrict__ AZI = p.f0.az_in + so;
     float *__restrict__ AXO = p.f0.ax_out + so;
     float *__restrict__ AZO = p.f0.az_out + so;
     const int64_t col = x + PAD, pitch = p.pitch;
-    const float dmx = __ldg(p.dampx + col);
-    const bool xin = x >= 4 && x < p.X - 4;
-    float w[8];
+    float dmx[4];
+    f4a(uld4(p.dampx + col), dmx);
+    float w[4][8];
 #pragma unroll
-    for (int k = 0; k < 7; k++)
-        w[k] = P[(int64_t)(z0 - 3 + k + PAD) * pitch + col];
-    const int nz = min(R, p.Z - z0);
-#pragma unroll 4
+    for (int k = 0; k < 7; k++) {
+        const float4 v = uld4(P + (int64_t)(z0 - 3 + k + PAD) * pitch + col);
+        w[0][k] = v.x;
+        w[1][k] = v.y;
+        w[2][k] = v.z;
+        w[3][k] = v.w;
+    }
+    const int nz = min(kURows, p.Z - z0);
+#pragma unroll 2
     for (int r = 0; r < nz; r++) {
         const int z = z0 + r;
         const int64_t o = (int64_t)(z + PAD) * pitch + col;
-        w[7] = P[o + 4 * pitch];
-        float u[8];
+        {
+            const float4 v = uld4(P + o + 4 * pitch);
+            w[0][7] = v.x;
+            w[1][7] = v.y;
+            w[2][7] = v.z;
+            w[3][7] = v.w;
+        }
+        float u[12], ax[4], az[4], nx[4], nzv[4];
+        f4a(uld4(P + o - 4), u);
+        f4a(uld4(P + o), u + 4);
+        f4a(uld4(P + o + 4), u + 8);
+        f4a(uld4(AXI + o), ax);
+        f4a(uld4(AZI + o), az);
+        const float dmz = __ldg(p.dampz + z + PAD);
+        const bool zin = z >= 4 && z < p.Z - 4;
 #pragma unroll
-        for (int k = 0; k < 8; k++)
-            u[k] = P[o - 3 + k];
-        float nx, nz_;
-        a_update(p, false, dmx, __ldg(p.dampz + z + PAD), ustag(u), ustag(w), AXI[o], AZI[o],
-                 xin && z >= 4 && z < p.Z - 4, nx, nz_);
-        AXO[o] = nx;
-        AZO[o] = nz_;
+        for (int j = 0; j < 4; j++) {
+            float dx, dz;
+            dstag_n<1>(u + j + 1, &dx);
+            dstag_n<1>(w[j], &dz);
+            a_update(p, false, dmx[j], dmz, dx, dz, ax[j], az[j], zin && x + j >= 4 && x + j < p.X - 4, nx[j],
+                     nzv[j]);
+        }
+        ust4(AXO + o, nx);
+        ust4(AZO + o, nzv);
 #pragma unroll
-        for (int k = 0; k < 7; k++)
-            w[k] = w[k + 1];
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int k = 0; k < 7; k++)
+                w[j][k] = w[j][k + 1];
     }
 }
 
 // Reverse A half-steps of both sets and the imaging condition: grid (ncb,
 // nseg, n_shots).
-template <int R>
-__global__ void __launch_bounds__(kUCols) k_unfused_a_rev(const __grid_constant__ UnfusedParams U)
+__global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_constant__ UnfusedParams U)
 {
     const StepParams &p = U.p;
-    const int x = blockIdx.x * kUCols + threadIdx.x;
+    const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= p.X)
         return;
-    const int shot = blockIdx.z, z0 = blockIdx.y * R;
+    const int shot = blockIdx.z, z0 = blockIdx.y * kURows;
     const int64_t so = p.shot_stride * shot;
     const float *__restrict__ PR = p.f0.px_out + so;
     const float *__restrict__ PA = p.f1.px_out + so;
     const int64_t col = x + PAD, pitch = p.pitch;
-    const float dmx = __ldg(p.dampx + col);
-    const bool xin = x >= 4 && x < p.X - 4;
-    float wr[9], wa[8];
+    float dmx[4];
+    f4a(uld4(p.dampx + col), dmx);
+    bool xin[4];
 #pragma unroll
-    for (int k = 0; k < 8; k++)
-        wr[k] = PR[(int64_t)(z0 - 4 + k + PAD) * pitch + col];
+    for (int j = 0; j < 4; j++)
+        xin[j] = x + j >= 4 && x + j < p.X - 4;
+    float wr[4][9], wa[4][8];
 #pragma unroll
-    for (int k = 0; k < 7; k++)
-        wa[k] = PA[(int64_t)(z0 - 3 + k + PAD) * pitch + col];
-    const int nz = min(R, p.Z - z0);
-#pragma unroll 2
+    for (int k = 0; k < 8; k++) {
+        const float4 v = uld4(PR + (int64_t)(z0 - 4 + k + PAD) * pitch + col);
+        wr[0][k] = v.x;
+        wr[1][k] = v.y;
+        wr[2][k] = v.z;
+        wr[3][k] = v.w;
+    }
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        const float4 v = uld4(PA + (int64_t)(z0 - 3 + k + PAD) * pitch + col);
+        wa[0][k] = v.x;
+        wa[1][k] = v.y;
+        wa[2][k] = v.z;
+        wa[3][k] = v.w;
+    }
+    const int nz = min(kURows, p.Z - z0);
     for (int r = 0; r < nz; r++) {
         const int z = z0 + r;
         const int64_t o = (int64_t)(z + PAD) * pitch + col;
-        const bool in = xin && z >= 4 && z < p.Z - 4;
-        wr[8] = PR[o + 4 * pitch];
-        wa[7] = PA[o + 4 * pitch];
-        // reconstruction: reverted A update and the Laplacian of P_rec(t)
-        float u[9];
+        const bool zin = z >= 4 && z < p.Z - 4;
+        {
+            const float4 v = uld4(PR + o + 4 * pitch);
+            wr[0][8] = v.x;
+            wr[1][8] = v.y;
+            wr[2][8] = v.z;
+            wr[3][8] = v.w;
+            const float4 a = uld4(PA + o + 4 * pitch);
+            wa[0][7] = a.x;
+            wa[1][7] = a.y;
+            wa[2][7] = a.z;
+            wa[3][7] = a.w;
+        }
+        float lap[4];
+        {
+            // reconstruction: reverted A update and the Laplacian of P_rec(t)
+            float u[12], ax[4], az[4], nx[4], nzv[4];
+            f4a(uld4(PR + o - 4), u);
+            f4a(uld4(PR + o), u + 4);
+            f4a(uld4(PR + o + 4), u + 8);
+            f4a(uld4(p.f0.ax_in + so + o), ax);
+            f4a(uld4(p.f0.az_in + so + o), az);
 #pragma unroll
-        for (int k = 0; k < 9; k++)
-            u[k] = PR[o - 4 + k];
-        float lx, lz;
-        lap_n<1>(u, &lx);
-        lap_n<1>(wr, &lz);
-        float nx, nz_;
-        a_update(p, true, 1.f, 1.f, ustag(u + 1), ustag(wr + 1), p.f0.ax_in[so + o], p.f0.az_in[so + o], in, nx,
-                 nz_);
-        p.f0.ax_out[so + o] = nx;
-        p.f0.az_out[so + o] = nz_;
-        // adjoint: damped A update and the imaging condition
-        float v[8];
+            for (int j = 0; j < 4; j++) {
+                float dx, dz, lx, lz;
+                dstag_n<1>(u + j + 1, &dx);
+                dstag_n<1>(wr[j] + 1, &dz);
+                lap_n<1>(u + j, &lx);
+                lap_n<1>(wr[j], &lz);
+                lap[j] = lap_combine(lx, lz);
+                a_update(p, true, 1.f, 1.f, dx, dz, ax[j], az[j], xin[j] && zin, nx[j], nzv[j]);
+            }
+            ust4(p.f0.ax_out + so + o, nx);
+            ust4(p.f0.az_out + so + o, nzv);
+        }
+        {
+            // adjoint: damped A update and the imaging condition
+            float u[12], ax[4], az[4], nx[4], nzv[4], g[4];
+            f4a(uld4(PA + o - 4), u);
+            f4a(uld4(PA + o), u + 4);
+            f4a(uld4(PA + o + 4), u + 8);
+            f4a(uld4(p.f1.ax_in + so + o), ax);
+            f4a(uld4(p.f1.az_in + so + o), az);
+            f4a(uld4c(p.grad + so + o), g);
+            const float dmz = __ldg(p.dampz + z + PAD);
 #pragma unroll
-        for (int k = 0; k < 8; k++)
-            v[k] = PA[o - 3 + k];
-        a_update(p, false, dmx, __ldg(p.dampz + z + PAD), ustag(v), ustag(wa), p.f1.ax_in[so + o],
-                 p.f1.az_in[so + o], in, nx, nz_);
-        p.f1.ax_out[so + o] = nx;
-        p.f1.az_out[so + o] = nz_;
-        p.grad[so + o] = __fmaf_rn(v[3], lap_combine(lx, lz), p.grad[so + o]);
+            for (int j = 0; j < 4; j++) {
+                float dx, dz;
+                dstag_n<1>(u + j + 1, &dx);
+                dstag_n<1>(wa[j], &dz);
+                a_update(p, false, dmx[j], dmz, dx, dz, ax[j], az[j], xin[j] && zin, nx[j], nzv[j]);
+                g[j] = __fmaf_rn(u[4 + j], lap[j], g[j]);
+            }
+            ust4(p.f1.ax_out + so + o, nx);
+            ust4(p.f1.az_out + so + o, nzv);
+            ust4(p.grad + so + o, g);
+        }
 #pragma unroll
-        for (int k = 0; k < 8; k++)
-            wr[k] = wr[k + 1];
+        for (int j = 0; j < 4; j++) {
 #pragma unroll
-        for (int k = 0; k < 7; k++)
-            wa[k] = wa[k + 1];
+            for (int k = 0; k < 8; k++)
+                wr[j][k] = wr[j][k + 1];
+#pragma unroll
+            for (int k = 0; k < 7; k++)
+                wa[j][k] = wa[j][k + 1];
+        }
     }
 }
 
-// Reverse: P_rec(t) = ring(T-1-t) on the ring cells: grid (ceil(n_ring /
-// 256), n_shots).
-__global__ void k_unfused_ring(const __grid_constant__ UnfusedParams U)
+// Point work between the P and A kernels, one thread per (cell, shot):
+// forward (RING = false): the sources fired by the shot, P += I (both split
+// components get I/2) and Q += I/2 on strip cells, in source order, after
+// the cell's P update, exactly as the fused kernels inject; reverse (RING):
+// P_rec(t) = ring(T-1-t) on the ring cells of set 0 and the adjoint sources
+// at the receivers into set 1. grid (ceil(n / 128), n_shots).
+__device__ __forceinline__ void inject_cell(const StepParams &p, const Fields &f, int shot, int off, const int *ids,
+                                            int e0, int e1, bool sources)
+{
+    const int64_t o = p.shot_stride * shot + off;
+    const int z = off / p.pitch - PAD, x = off - (z + PAD) * p.pitch - PAD;
+    const bool strip = __ldg(p.dampx + x + PAD) != 1.f || __ldg(p.dampz + z + PAD) != 1.f;
+    float pn = f.px_out[o], qn = strip ? f.pz_out[o] : 0.f;
+    for (int e = e0; e < e1; e++) {
+        const int row = sources ? p.fire_row[shot * p.n_src + ids[e]] : shot * p.n_sen + ids[e];
+        if (row < 0)
+            continue;
+        const float I = p.inj_tab[(int64_t)row * p.T + p.t];
+        pn = __fadd_rn(pn, I);
+        if (strip)
+            qn = __fadd_rn(qn, __fmul_rn(I, 0.5f));
+    }
+    f.px_out[o] = pn;
+    if (strip)
+        f.pz_out[o] = qn;
+}
+
+template <bool RING>
+__global__ void __launch_bounds__(128) k_unfused_points(const __grid_constant__ UnfusedParams U)
 {
     const StepParams &p = U.p;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.n_ring)
-        return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int shot = blockIdx.y;
-    p.f0.px_out[p.shot_stride * shot + U.ring_off[k]] =
-        p.ring[((int64_t)shot * p.T + (p.T - 1 - p.t)) * p.n_ring + k];
+    if (!RING) {
+        if (i < U.n_src_cells)
+            inject_cell(p, p.f0, shot, U.src_off[i], U.src_id, U.src_ptr[i], U.src_ptr[i + 1], true);
+        return;
+    }
+    if (i < p.n_ring) {
+        p.f0.px_out[p.shot_stride * shot + U.ring_off[i]] =
+            p.ring[((int64_t)shot * p.T + (p.T - 1 - p.t)) * p.n_ring + i];
+        return;
+    }
+    const int k = i - p.n_ring;
+    if (k < U.n_rcv_cells)
+        inject_cell(p, p.f1, shot, U.rcv_off[k], U.rcv_id, U.rcv_ptr[k], U.rcv_ptr[k + 1], false);
 }
 
 }  // namespace otf

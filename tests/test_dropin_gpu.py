@@ -180,6 +180,33 @@ def test_streaming_kernels_close_to_oracle(lib, rows):
         os.environ.pop("OTFWI_STREAM_ROWS", None)
 
 
+def test_unfused_kernels_close_to_oracle(lib):
+    """Unfused streaming half-steps (kernel 4): within the fast-mode tolerance
+    of the FP64 oracle on the medium case, the strip case and grids whose
+    width is not a multiple of the 128-column block or of 4; identical to the
+    strip-split kernels (with dt = dx the damped and undamped A updates round
+    the same way, so the two compute the same operations)."""
+    import make_sim_golden
+    from otfwi_b200 import scenarios
+    from otfwi_b200.cuda_interface_pml import pml_damping
+    cases = [("medium", _cases()["medium"]), ("strip", _strip_case())]
+    for X, Z, seed in ((268, 84, 12), (101, 77, 3)):
+        sc = scenarios.small(X=X, Z=Z, T=220, n_src=2, n_rec=7, seed=seed, f0=0.05)
+        cases.append((f"{X}x{Z}", make_sim_golden.case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))))
+    for name, inp in cases:
+        res = _run(lib, inp, precision=1, kernel=4)
+        ref64 = oracle_case(inp, "f64")
+        fam = lambda k: k.rstrip("0123456789")
+        scale = {}
+        for k in _keys(ref64):
+            scale[fam(k)] = max(scale.get(fam(k), 0.0), float(np.abs(ref64[k]).max()))
+        for k in _keys(ref64):
+            a, b = np.asarray(res[k], np.float64), np.asarray(ref64[k])
+            assert np.abs(a - b).max() <= 1e-4 * scale[fam(k)], (name, k)
+        ref = _run(lib, inp, precision=1, tile=4, kernel=2)
+        _assert_identical(res, ref, f"unfused vs strip-split {name}")
+
+
 def test_odd_grid_sizes_every_tile(lib):
     """Grids that are not multiples of any tile shape, both kernel variants."""
     import make_sim_golden
