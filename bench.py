@@ -324,7 +324,9 @@ def run_ours(args):
                 "roofline": roof, "e2e": e2e,
                 # per step: T-1 forward + T-1 reverse step kernels, misfit,
                 # misfit sum, adjoint running integral, shot mean
-                "gpu_launches": args.steps * (2 * (sc.T - 1) + 4),
+                # per time step: one fused launch forward and one reverse; the
+                # unfused variant 4 has P, point and A launches in each
+                "gpu_launches": args.steps * ((6 if args.kernel == 4 else 2) * (sc.T - 1) + 4),
                 "clocks": clk.summary(),
                 "misfit_value": float(mis.item())}
         if not args.no_cpu_baseline:

@@ -137,7 +137,8 @@ int otf_batch_forward_ring(otf_batch *b, float *traces, int on_device);
 /* Full gradient: forward, device misfit (0 = L2, 1 = Wasserstein as
  * adjoint_functions.wasserstein, 2 = Wasserstein on softplus-normalised
  * traces, 3 = adjoint_functions.wasserstein_quad, 4 = adjoint_functions.
- * quad_envelope), reverse phase; grad [Z*X]
+ * quad_envelope, 5 = adjoint_functions.wasserstein_pm with its negative-part
+ * CDFs taken from the negative parts), reverse phase; grad [Z*X]
  * = mean over shots of the per-shot gradients, *misfit = sum over every
  * trace (both optional). */
 int otf_batch_gradient(otf_batch *b, int misfit_kind, float *grad, double *misfit, int on_device);

@@ -7,6 +7,9 @@ imports it.
 Restates the reference's ``adjoint_functions.py`` (Otfwi project root):
   * ``L2``          adjoint_functions.py:8-11
   * ``wasserstein`` adjoint_functions.py:25-67 (the misfit regression.py:42 uses)
+  * ``wasserstein_quad`` adjoint_functions.py:70-104, ``wasserstein_pm``
+    adjoint_functions.py:144-223 (as written, and with its G_n / F_n lines
+    taking the negative parts), ``quad_envelope`` adjoint_functions.py:14-22
 
 The reference computes through two scipy routines that are not part of the
 reference tree (scipy 1.18.1 is the version installed beside it). Their
@@ -229,3 +232,65 @@ def quad_envelope(sim, obs):
     e = np.abs(hs) ** 2 - np.abs(ho) ** 2
     adj = np.asarray(sim, np.float64) * e - np.imag(analytic_signal(e * np.imag(hs)))
     return np.sum(e ** 2), adj
+
+
+def wasserstein_pm_trace(sim_s, obs_s, t, dt, fixed=True):
+    """One trace of adjoint_functions.py:144-223 (wasserstein_pm): the positive
+    and the negative parts of each trace as two densities, each shifted by 1%
+    of the observed part's maximum, rectangle-normalised, rectangle-rule CDFs;
+    misfit sum (F_p^-1 - G_p^-1)^2 + sum (F_n^-1 - G_n^-1)^2, adjoint the
+    sum of the two transport potentials cumsum(t - G^-1(F(t))) dt, less its
+    last value. The reference builds G_n and F_n from the POSITIVE parts
+    (adjoint_functions.py:179-180), which makes the negative part vanish from
+    the result; ``fixed=False`` reproduces that line as written, ``fixed=True``
+    (the device misfit) uses the negative parts. Each operation keeps the
+    reference's dtype: the observed parts are float32 and normalised in
+    place, the simulated ones float64; the two misfit sums are Python sums."""
+    g_p = np.maximum(0, obs_s)
+    f_p = np.maximum(0, sim_s)
+    g_n = -np.minimum(0, obs_s)
+    f_n = -np.minimum(0, sim_s)
+    c_p = np.max(g_p) * 0.01
+    c_n = np.max(g_n) * 0.01
+    g_p += c_p
+    f_p += c_p
+    g_n += c_n
+    f_n += c_n
+    mass_gp = np.sum(g_p * dt)
+    mass_gn = np.sum(g_n * dt)
+    mass_fp = np.sum(f_p * dt)
+    mass_fn = np.sum(f_n * dt)
+    g_p /= mass_gp
+    g_n /= mass_gn
+    f_p /= mass_fp
+    f_n /= mass_fn
+    G_p = np.cumsum(g_p * dt)
+    F_p = np.cumsum(f_p * dt)
+    G_n = np.cumsum((g_n if fixed else g_p) * dt)
+    F_n = np.cumsum((f_n if fixed else f_p) * dt)
+    F_ip = Interp1dLinear(t, F_p)
+    G_1p = Interp1dLinear(G_p, t)
+    F_1p = Interp1dLinear(F_p, t)
+    F_in = Interp1dLinear(t, F_n)
+    G_1n = Interp1dLinear(G_n, t)
+    F_1n = Interp1dLinear(F_n, t)
+    dist = Interp1dLinear(t, np.cumsum(t - G_1p(F_ip(t))) * dt + np.cumsum(t - G_1n(F_in(t))) * dt)
+    adj = dist(t) - dist(t[-1])
+    w2 = sum(np.abs(F_1p(t) - G_1p(t)) ** 2) + sum(np.abs(F_1n(t) - G_1n(t)) ** 2)
+    return w2, adj
+
+
+def wasserstein_pm(sim, obs, fixed=True):
+    """adjoint_functions.py:144-223 over every trace (see wasserstein_pm_trace)."""
+    sim = np.asarray(sim)
+    obs = np.asarray(obs)
+    n_sens, T = sim.shape
+    t = np.linspace(0, 1, T)
+    dt = t[1] - t[0]
+    W2 = 0
+    s_W2 = np.zeros((n_sens, T))
+    for s in range(n_sens):
+        w2, adj = wasserstein_pm_trace(sim[s].copy(), obs[s].copy(), t, dt, fixed)
+        s_W2[s, :] = adj
+        W2 += w2
+    return W2, s_W2

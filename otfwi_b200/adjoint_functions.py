@@ -11,6 +11,9 @@ init_regression`` as the adjoint callback:
                         reference counterpart; definition in misfit.cu)
   wasserstein_quad      adjoint_functions.py:70-108
   quad_envelope         adjoint_functions.py:14-22
+  wasserstein_pm        adjoint_functions.py:144-223, its negative-part CDFs
+                        built from the negative parts (lines 179-180 of the
+                        reference take the positive ones)
 
 The arithmetic runs in the library's misfit kernels (otf_misfit); device
 memory comes from PyTorch. No CPU fallback: without a GPU these raise.
@@ -66,3 +69,7 @@ def wasserstein_quad(sim, obs):
 
 def quad_envelope(sim, obs):
     return _device_misfit(MISFITS["quad_envelope"], sim, obs)
+
+
+def wasserstein_pm(sim, obs):
+    return _device_misfit(MISFITS["wasserstein_pm"], sim, obs)

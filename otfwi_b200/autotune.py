@@ -34,9 +34,9 @@ def cache_path():
                           os.path.join(os.path.expanduser("~"), ".cache", "otfwi_b200", "tune.json"))
 
 
-def _key(X, Z, shots, n_rec, precision, gpu):
-    cands = ",".join(f"{k}/{t}" for k, t in candidates(precision))
-    return f"{gpu}|{X}x{Z}|shots{shots}|rx{n_rec}|prec{precision}|{cands}"
+def _key(X, Z, shots, n_rec, precision, gpu, cands):
+    tried = ",".join(f"{k}/{t}" for k, t in cands)
+    return f"{gpu}|{X}x{Z}|shots{shots}|rx{n_rec}|prec{precision}|{tried}"
 
 
 def _load():
@@ -92,13 +92,14 @@ def autotune(sc, precision=1, misfit="wasserstein_softplus", T_proxy=300, use_ca
     ``cands``: [(kernel, tile)] to try instead of every compiled candidate."""
     import torch
     gpu = torch.cuda.get_device_name()
-    key = _key(sc.X, sc.Z, sc.n_src, sc.n_rec, precision, gpu)
+    cands = cands if cands is not None else candidates(precision)
+    key = _key(sc.X, sc.Z, sc.n_src, sc.n_rec, precision, gpu, cands)
     cache = _load() if use_cache else {}
     if key in cache:
         e = cache[key]
         return e["kernel"], e["tile"], e.get("table", {})
     table = {}
-    for kernel, tile in (cands if cands is not None else candidates(precision)):
+    for kernel, tile in cands:
         t0 = time.perf_counter()
         try:
             ms = time_config(sc, kernel, tile, precision, T_proxy, misfit)

@@ -18,7 +18,8 @@ import numpy as np
 from . import _lib
 from .cuda_interface_pml import pml_damping, ring_mask
 
-MISFITS = {"l2": 0, "wasserstein": 1, "wasserstein_softplus": 2, "wasserstein_quad": 3, "quad_envelope": 4}
+MISFITS = {"l2": 0, "wasserstein": 1, "wasserstein_softplus": 2, "wasserstein_quad": 3, "quad_envelope": 4,
+           "wasserstein_pm": 5}
 
 
 def _declare(lib):

@@ -940,7 +940,8 @@ StepParams Engine::base_params() const
 // Kernel variant actually used: the requested one where compiled for the
 // tile shape and numerics, else the next simpler one (2 -> 1 -> 0). The
 // strip-split kernels (2) implement the fast numerics only; -1 = automatic
-// (2 for fast, 1 for faithful).
+// (4, the unfused kernels, for fast numerics with separable damping, else 2
+// for fast, 1 for faithful).
 static int resolve_variant(const KernelSet &k, int requested, int precision)
 {
     int v = requested < 0 ? (precision == kFast ? 2 : 1) : requested;
@@ -956,7 +957,9 @@ int Engine::variant_in_use() const
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
     if (variant_ == 3 && cfg_.precision == kFast && sep_ && cfg_.X % 4 == 0)
         return 3;
-    if (variant_ == 4 && cfg_.precision == kFast && sep_)
+    // the unfused streaming half-steps are the default of the fast numerics
+    // (separable damping), measured fastest on every grid tried
+    if ((variant_ == 4 || variant_ < 0) && cfg_.precision == kFast && sep_)
         return 4;
     return resolve_variant(k, variant_ >= 3 ? 2 : variant_, cfg_.precision);
 }

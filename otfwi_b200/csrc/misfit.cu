@@ -9,6 +9,12 @@
 //  kind 2  Wasserstein on softplus-normalised traces (no reference counterpart):
 //                       p = phi(f)/Z, phi = s softplus(./s), s = 0.1 max|obs|,
 //                       same W2 and potential, adjoint through phi and Z
+//  kind 3  wasserstein_quad  adjoint_functions.py:70-104 (squared traces)
+//  kind 5  wasserstein_pm    adjoint_functions.py:144-223 with its negative-part
+//                       CDFs built from the negative parts (the reference's
+//                       lines 179-180 take the positive ones): positive and
+//                       negative parts as two densities, W2 and transport
+//                       potentials summed over both
 //
 // The reference evaluates kinds 0/1 in FP64 on the host. Here every
 // accumulation (normalisation sums, the two CDF scans, the misfit sum, the
@@ -383,6 +389,89 @@ __global__ void __launch_bounds__(MT) k_wasserstein(const float *__restrict__ si
         misfit[tr] = ff2d(w2);
 }
 
+// wasserstein_pm (kind 5): per part (positive, negative) the observed
+// density max(0, +-obs) + c (c = 1% of the observed part's maximum, FP32 as
+// NumPy keeps float32 * Python float) normalised in place in FP32, the
+// simulated one max(0, +-sim) + c in FP64 class; rectangle CDFs cumsum(p dt);
+// W2 = sum (F^-1(t) - G^-1(t))^2 over both parts; adjoint = the summed
+// potentials cumsum(t - G^-1(F(t))) dt, less their last value. Every CDF is
+// strictly increasing (c > 0), so no sort is needed.
+__global__ void __launch_bounds__(MT) k_wasserstein_pm(const float *__restrict__ sim, const float *__restrict__ obs,
+                                                       float *__restrict__ adj, double *__restrict__ misfit,
+                                                       char *scratch, int T, int64_t per_trace)
+{
+    __shared__ FF red[MT / 32];
+    __shared__ float redf[MT / 32];
+    const int tr = blockIdx.x;
+    const float *f = sim + (int64_t)tr * T;
+    const float *g = obs + (int64_t)tr * T;
+    FF *Fp = reinterpret_cast<FF *>(scratch + per_trace * tr);
+    FF *Gp = Fp + T, *Fn = Gp + T, *Gn = Fn + T, *V = Gn + T;
+    const double step = 1.0 / (double)(T - 1);
+    float mp = 0.f, mn = 0.f, af = 0.f;
+    for (int i = threadIdx.x; i < T; i += MT) {
+        mp = fmaxf(mp, g[i]);
+        mn = fmaxf(mn, -g[i]);
+        af = fmaxf(af, fabsf(f[i]));
+    }
+    mp = block_minmax(mp, true, redf);
+    mn = block_minmax(mn, true, redf);
+    af = block_minmax(af, true, redf);
+    const float cp = __fmul_rn(mp, 0.01f), cn = __fmul_rn(mn, 0.01f);
+    // exact power-of-two scaling to unit magnitude (the densities are
+    // normalised, so it cancels; float-float needs normal magnitudes)
+    float scale = 1.f;
+    {
+        const double m = fmax(fmax((double)mp, (double)mn), (double)af);
+        if (m > 0.0 && m < 1e30)
+            scale = ldexpf(1.f, -ilogb(m));
+    }
+    const float cps = __fmul_rn(cp, scale), cns = __fmul_rn(cn, scale);
+    auto gpv = [&](int i) { return __fmul_rn(__fadd_rn(fmaxf(g[i], 0.f), cp), scale); };
+    auto gnv = [&](int i) { return __fmul_rn(__fadd_rn(fmaxf(-g[i], 0.f), cn), scale); };
+    auto fpv = [&](int i) { return add(ff(__fmul_rn(fmaxf(f[i], 0.f), scale)), ff(cps)); };
+    auto fnv = [&](int i) { return add(ff(__fmul_rn(fmaxf(-f[i], 0.f), scale)), ff(cns)); };
+    FF sgp{0.f, 0.f}, sgn{0.f, 0.f}, sfp{0.f, 0.f}, sfn{0.f, 0.f};
+    for (int i = threadIdx.x; i < T; i += MT) {
+        sgp = add(sgp, ff(gpv(i)));
+        sgn = add(sgn, ff(gnv(i)));
+        sfp = add(sfp, fpv(i));
+        sfn = add(sfn, fnv(i));
+    }
+    const FF dtf = ffd(step);
+    const FF Zgp = mul(block_sum(sgp, red), dtf), Zgn = mul(block_sum(sgn, red), dtf);
+    const FF Zfp = mul(block_sum(sfp, red), dtf), Zfn = mul(block_sum(sfn, red), dtf);
+    block_scan(Gp, T, [&](int i) -> FF { return mul(ff(__double2float_rn(ff2d(div(ff(gpv(i)), Zgp)))), dtf); },
+               red);
+    block_scan(Gn, T, [&](int i) -> FF { return mul(ff(__double2float_rn(ff2d(div(ff(gnv(i)), Zgn)))), dtf); },
+               red);
+    block_scan(Fp, T, [&](int i) -> FF { return mul(div(fpv(i), Zfp), dtf); }, red);
+    block_scan(Fn, T, [&](int i) -> FF { return mul(div(fnv(i), Zfn), dtf); }, red);
+    auto inv = [&](const FF *C, FF q) {  // interp1d(C, t) at q
+        const int j = search_left(C, T, q);
+        return lerp(q, C[j - 1], C[j], ffd(tval(j - 1, T, step)), ffd(tval(j, T, step)));
+    };
+    FF w2p{0.f, 0.f}, w2n{0.f, 0.f};
+    for (int i = threadIdx.x; i < T; i += MT) {
+        const FF ti = ffd(tval(i, T, step));
+        const FF dp = sub(inv(Fp, ti), inv(Gp, ti));
+        const FF dn = sub(inv(Fn, ti), inv(Gn, ti));
+        w2p = add(w2p, mul(dp, dp));
+        w2n = add(w2n, mul(dn, dn));
+        V[i] = add(sub(ti, inv(Gp, Fp[i])), sub(ti, inv(Gn, Fn[i])));
+    }
+    w2p = block_sum(w2p, red);
+    w2n = block_sum(w2n, red);
+    __syncthreads();
+    block_scan(V, T, [&](int i) -> FF { return mul(V[i], dtf); }, red);
+    const FF last = V[T - 1];
+    float *a = adj + (int64_t)tr * T;
+    for (int i = threadIdx.x; i < T; i += MT)
+        a[i] = __double2float_rn(ff2d(sub(V[i], last)));
+    if (threadIdx.x == 0)
+        misfit[tr] = ff2d(w2p) + ff2d(w2n);
+}
+
 // L2: adj = sim - obs in FP64 rounded to FP32 (the reference's float64
 // residual written into the FP32 adjoint buffer); misfit = sum r^2 in FP64.
 __global__ void __launch_bounds__(MT) k_l2(const float *__restrict__ sim, const float *__restrict__ obs,
@@ -420,6 +509,8 @@ int64_t misfit_scratch_per_trace(int kind, int T)
         return 0;
     if (kind == kMisfitQuadEnvelope)
         return envelope_scratch_per_trace(T);
+    if (kind == kMisfitWassersteinPM)
+        return ((int64_t)sizeof(FF) * 5 * T + 255) / 256 * 256;
     int64_t P = 1;
     while (P < T)
         P <<= 1;
@@ -450,6 +541,9 @@ int launch_misfit(int kind, const float *sim, const float *obs, float *adj, doub
         return launch_envelope(sim, obs, adj, misfit, n_traces, T, scratch, st);
     case kMisfitWassersteinQuad:
         k_wasserstein<3><<<n_traces, MT, 0, st>>>(sim, obs, adj, misfit, (char *)scratch, T, per);
+        break;
+    case kMisfitWassersteinPM:
+        k_wasserstein_pm<<<n_traces, MT, 0, st>>>(sim, obs, adj, misfit, (char *)scratch, T, per);
         break;
     default:
         OTF_CHECK(false, 1, "misfit: unknown kind");

@@ -10,9 +10,10 @@ enum MisfitKind : int {
     kMisfitWasserstein = 1,
     kMisfitWassersteinSoftplus = 2,
     kMisfitWassersteinQuad = 3,
-    kMisfitQuadEnvelope = 4
+    kMisfitQuadEnvelope = 4,
+    kMisfitWassersteinPM = 5
 };
-constexpr int kNumMisfits = 5;
+constexpr int kNumMisfits = 6;
 
 // quad_envelope (envelope.cu): FFT plans are created by envelope_prepare,
 // which must run outside stream capture (plan creation allocates).

@@ -83,7 +83,8 @@ def build(spec, sc, misfit, tune):
     from .autotune import autotune
     kernel, tile = -1, 4
     if tune:
-        kernel, tile, _ = autotune(sc, precision=1, misfit=misfit, T_proxy=150, cands=[(2, 0), (2, 1), (2, 4)])
+        kernel, tile, _ = autotune(sc, precision=1, misfit=misfit, T_proxy=150,
+                                  cands=[(4, 4), (2, 0), (2, 1), (2, 4)])
     b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, precision=1, tile=tile,
                   kernel=kernel)
     b.set_model(sc.c_true)

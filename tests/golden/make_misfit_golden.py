@@ -9,8 +9,9 @@ import shims the installed environment needs:
 Inputs are seeded synthetic traces with the shape of recorded ultrasonic
 A-scans (Ricker-like pulses with travel-time shifts and noise), stored as
 float32 like the simulator's recordings. The outputs are the reference's
-(W2, adjoint source), (L2, residual), wasserstein_quad's (W2, adjoint) and
-quad_envelope's (misfit, adjoint).
+(W2, adjoint source), (L2, residual), wasserstein_quad's (W2, adjoint),
+quad_envelope's (misfit, adjoint) and wasserstein_pm's (W2, adjoint), the
+last as written (its negative-part CDFs are built from the positive parts).
 
     python tests/golden/make_misfit_golden.py --ref /path/to/Otfwi
 """
@@ -82,10 +83,11 @@ def main():
         l2, resid = adj.L2(sim.astype(np.float64), obs)
         w2q, s_w2q = adj.wasserstein_quad(sim.astype(np.float64), obs)
         env, env_adj = adj.quad_envelope(sim.astype(np.float64), obs)
+        w2pm, s_w2pm = adj.wasserstein_pm(sim.astype(np.float64), obs)
         path = os.path.join(args.out, f"misfit_{name}.npz")
         np.savez_compressed(path, sim=sim, obs=obs, w2=np.float64(w2), w2_adj=s_w2,
                             l2=np.float64(l2), l2_adj=resid, w2q=np.float64(w2q), w2q_adj=s_w2q,
-                            env=np.float64(env), env_adj=env_adj)
+                            env=np.float64(env), env_adj=env_adj, w2pm=np.float64(w2pm), w2pm_adj=s_w2pm)
         print(path, sim.shape, float(w2), float(l2))
 
 

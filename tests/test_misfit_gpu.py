@@ -66,6 +66,40 @@ def test_device_quad_envelope(lib, path):
     assert _rel_max(adj, d["env_adj"]) <= 1e-5
 
 
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "misfit_*.npz"))),
+                         ids=os.path.basename)
+def test_device_wasserstein_pm(lib, path):
+    """wasserstein_pm with its negative-part CDFs from the negative parts,
+    against the oracle of that form (whose as-written form reproduces the
+    reference bit for bit, tests/test_oracle.py), to the Wasserstein kinds'
+    tolerance; and through the batched gradient graph (kind 5)."""
+    from otfwi_b200.batch import device_misfit
+    d = np.load(path)
+    w2, ref = mo.wasserstein_pm(d["sim"].astype(np.float64), d["obs"], fixed=True)
+    m, adj = device_misfit(d["sim"], d["obs"], "wasserstein_pm")
+    assert abs(m.sum() - w2) <= 1e-5 * abs(w2), (m.sum(), w2)
+    assert _rel_max(adj, ref) <= 1e-5
+
+
+def test_batched_gradient_with_wasserstein_pm(lib):
+    """The gradient graph with misfit kind 5: the misfit it reports equals the
+    stand-alone device misfit of the same traces."""
+    from otfwi_b200 import scenarios
+    from otfwi_b200.batch import ShotBatch, device_misfit
+    sc = scenarios.small(X=128, Z=96, T=300, n_src=3, n_rec=10, seed=21, f0=0.035)
+    b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, precision=1)
+    b.set_model(sc.c_true)
+    obs = b.forward()
+    b.set_observed(obs)
+    b.set_model(sc.c_start)
+    sim = b.forward()
+    g, mis = b.gradient("wasserstein_pm")
+    m, _ = device_misfit(sim.reshape(-1, sc.T), obs.reshape(-1, sc.T), "wasserstein_pm")
+    assert np.isfinite(g).all() and np.abs(g).max() > 0
+    assert abs(mis - m.sum()) <= 1e-12 * abs(m.sum())
+    b.close()
+
+
 def test_wasserstein_long_traces_and_many(lib):
     """T = 4000 traces (the FMC length), many traces in one launch."""
     from otfwi_b200.batch import device_misfit

@@ -38,6 +38,20 @@ def test_misfit_oracle_matches_reference_bit_exact(path):
 
 
 @pytest.mark.parametrize("path", _misfit_cases(), ids=os.path.basename)
+def test_wasserstein_pm_oracle_matches_reference_bit_exact(path):
+    """The oracle of adjoint_functions.wasserstein_pm as written (its G_n / F_n
+    built from the positive parts) reproduces the reference bit for bit; the
+    fixed form differs from it only through the negative parts."""
+    d = np.load(path)
+    sim = d["sim"].astype(np.float64)
+    w2, adj = mo.wasserstein_pm(sim, d["obs"], fixed=False)
+    assert w2 == d["w2pm"]
+    assert np.array_equal(adj, d["w2pm_adj"])
+    w2f, adjf = mo.wasserstein_pm(sim, d["obs"], fixed=True)
+    assert w2f != w2 and np.all(np.isfinite(adjf))
+
+
+@pytest.mark.parametrize("path", _misfit_cases(), ids=os.path.basename)
 def test_quad_envelope_oracle_vs_reference(path):
     """The reference's analytic signal of the float32 observed trace goes
     through scipy.fft in single precision; the oracle's is FP64, so the two
