@@ -36,6 +36,7 @@ UNIT = "Gcell-steps/s"
 BYTES_FWD = 28
 BYTES_REV = 64
 BYTES_STEP = 92
+BYTES_AREV = 48  # k_unfused_a_rev: both sets' P, Ax, Az and grad read; four A fields and grad written
 
 
 def parse():
@@ -139,12 +140,18 @@ def profile_traffic(kernel):
     profiles/reverse_step_fmc.md for the fused strip-split step (one
     launch), profiles/reverse_step_unfused_fmc.md for the unfused one (its
     three launches summed)."""
+    return profile_value(kernel, "dram_bytes_per_cell")
+
+
+def profile_value(kernel, key):
+    """A 'key: N' line of the committed ncu summary of the reverse step of
+    this kernel variant (None when absent)."""
     name = "reverse_step_unfused_fmc.md" if kernel == 4 else "reverse_step_fmc.md"
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.strip().startswith("dram_bytes_per_cell:"):
+        if line.strip().startswith(key + ":"):
             return float(line.split(":")[1])
     return None
 
@@ -262,7 +269,7 @@ def run_ours(args):
     ach_fwd = BYTES_FWD * per_launch_cells / (ms_fwd / 1e3) / 1e9
     tr = profile_traffic(args.kernel)
     if args.kernel == 4:
-        rev_name = ("reverse step (k_unfused_p_rev + k_unfused_ring + k_unfused_a_rev: adjoint + "
+        rev_name = ("reverse step (k_unfused_p_rev + k_unfused_points<1> + k_unfused_a_rev: adjoint + "
                     "reconstruction + imaging condition, all shots; 88 B/cell moved)")
     else:
         rev_name = "k_reverse_split (adjoint + reconstruction + imaging condition, all shots)"
@@ -277,6 +284,17 @@ def run_ours(args):
                                "algorithmic_bytes_per_launch": BYTES_FWD * per_launch_cells},
             "whole_step_frac": round(BYTES_STEP * sc.X * sc.Z * (sc.T - 1) * sc.n_src
                                      / (ms / 1e3) / 1e9 / peak, 4)}
+    share = profile_value(args.kernel, "a_rev_share_of_step") if args.kernel == 4 else None
+    if share:
+        # the largest single kernel of the unfused reverse step; its time is the
+        # step's live CUDA-event time times its share of the step in the
+        # committed launch list (a graph's kernels cannot be timed one by one)
+        ms_a = ms_rev * share
+        ach_a = BYTES_AREV * per_launch_cells / (ms_a / 1e3) / 1e9
+        roof["dominant_kernel"] = {"name": "k_unfused_a_rev", "algorithmic_bytes_per_launch":
+                                   BYTES_AREV * per_launch_cells, "launch_ms_est": round(ms_a, 4),
+                                   "share_of_step": share, "achieved": round(ach_a, 1),
+                                   "frac": round(ach_a / peak, 4)}
 
     # end to end through the public API with host buffers: model and
     # observed traces from pinned host memory, gradient and misfit back
