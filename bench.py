@@ -15,6 +15,7 @@ Metric: fwd+adj Gcell-steps/s = 2 * X * Z * (T-1) * shots / step time
 or --impl reference for the reference library's per-shot loop.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -57,6 +58,11 @@ def parse():
     ap.add_argument("--misfit", default="wasserstein_softplus")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-shots", type=int, default=2, help="shots per reference-arm step")
+    ap.add_argument("--leg", default="gradient", choices=["gradient", "cpml", "misfits"],
+                    help="gradient: the headline FMC gradient (default); cpml: the second-order CPML "
+                         "path, this library against the reference's; misfits: the device trace misfits "
+                         "against the CPU restatement")
+    ap.add_argument("--cpml-impl", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -340,10 +346,9 @@ def run_ours(args):
                                kernel_variant=args.kernel, tile=args.tile, autotune=tuned,
                                stream_rows=args.stream_rows if args.kernel == 3 else None),
                 "roofline": roof, "e2e": e2e,
-                # per step: T-1 forward + T-1 reverse step kernels, misfit,
-                # misfit sum, adjoint running integral, shot mean
-                # per time step: one fused launch forward and one reverse; the
-                # unfused variant 4 has P, point and A launches in each
+                # per time step one fused launch forward and one reverse (the
+                # unfused variant 4: P, point and A launches in each); per
+                # gradient the misfit, its sum, the running integral, shot mean
                 "gpu_launches": args.steps * ((6 if args.kernel == 4 else 2) * (sc.T - 1) + 4),
                 "clocks": clk.summary(),
                 "misfit_value": float(mis.item())}
@@ -415,9 +420,143 @@ def run_reference(args):
                               "d2h_bytes_per_step": 0}}), flush=True)
 
 
+def cpml_case(args):
+    """The CPML leg's workload: a 512x512 seeded model (scenarios.small's
+    layered velocity with density 1-1.5), 8 sources firing together, 64
+    receivers, T steps; the CPML profiles built by otfwi_b200.cpml."""
+    from otfwi_b200 import scenarios
+    sc = scenarios.small(X=args.X, Z=args.X, T=args.T, n_src=8, n_rec=64, seed=31, f0=0.02)
+    rho = 1.0 + 0.5 * np.random.default_rng(31).random((sc.Z, sc.X))
+    return sc, rho
+
+
+def run_cpml_impl(args):
+    """One library's CPML forward (and, for this library, its exact adjoint)
+    timed in this process; prints a JSON fragment. The reference's library
+    resets the device on init, so each library runs in its own process."""
+    from otfwi_b200.cpml import CPML_LIB, CPMLSimulator
+    sc, rho = cpml_case(args)
+    lib = CPML_LIB if args.cpml_impl == "ours" else os.path.join(ROOT, "oracle", "_ref", "cuda_regression_CPML.so")
+    if not os.path.exists(lib):
+        print(json.dumps({"unavailable": f"{os.path.relpath(lib, ROOT)} not built"}))
+        return
+    sim = CPMLSimulator(sc.X, sc.Z, sc.T, sc.PML, sc.c_true, sc.src_mask, sc.rec_mask, sc.source, rho=rho,
+                        f0=0.02, lib=lib)
+    for _ in range(args.warmup):
+        rec = sim.simulate(-1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rec = sim.simulate(-1)
+    dt = (time.perf_counter() - t0) / args.steps
+    out = {"forward_s": dt, "forward_gcell_steps_per_s": sc.X * sc.Z * (sc.T - 1) / dt / 1e9,
+           "traces_max": float(np.abs(rec).max())}
+    if args.cpml_impl == "ours":
+        g = np.asarray(rec, np.float32) * 1e-3
+        sim.gradient(g)
+        t0 = time.perf_counter()
+        sim.gradient(g)
+        out["gradient_s"] = time.perf_counter() - t0
+    print(json.dumps(out), flush=True)
+
+
+def run_cpml_leg(args):
+    """CPML path (regression_CPML.cu): this library's forward against the
+    reference's own library on the same inputs, each through its C ABI and
+    timed around cuda_simulate2 (traces copied back, as the ABI returns
+    them); the exact adjoint of this library beside it (the reference has
+    none)."""
+    import subprocess
+    res = {}
+    for impl in ("ours", "reference"):
+        cmd = [sys.executable, os.path.abspath(__file__), "--leg", "cpml", "--cpml-impl", impl, "--X",
+               str(args.X), "--T", str(args.T), "--steps", str(args.steps), "--warmup", str(args.warmup)]
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+        lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+        res[impl] = json.loads(lines[-1]) if lines else {"unavailable": out.stderr.strip()[-300:]}
+    ours = res["ours"].get("forward_gcell_steps_per_s")
+    ref = res["reference"].get("forward_gcell_steps_per_s")
+    print(json.dumps({"metric": "CPML forward Gcell-steps/s", "value": ours, "unit": "Gcell-steps/s",
+                      "leg": "cpml", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "higher_is_better": True, "data": "synthetic",
+                      "config": {"workload": f"cpml{args.X}x{args.X}_T{args.T}_8src_64rx"},
+                      "reference_value": ref, "speedup": (ours / ref) if ours and ref else None,
+                      "ours": res["ours"], "reference": res["reference"]}), flush=True)
+
+
+def run_misfit_leg(args):
+    """Device trace misfits: every kind on the FMC workload's trace count
+    (shots x receivers x T), timed with CUDA events, against the CPU
+    restatement (oracle/misfit_oracle.py, the reference's numpy recipes)
+    timed on a sample of traces."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import misfit_oracle as mo
+    from otfwi_b200.batch import MISFITS, _declare
+    from otfwi_b200 import _lib
+    L = _declare(_lib.load())
+    rng = np.random.default_rng(7)
+    n, T = args.shots * args.shots, args.T
+    t = np.arange(T)
+    sim = np.zeros((n, T), np.float32)
+    obs = np.zeros((n, T), np.float32)
+    for i in range(n):
+        t1 = rng.uniform(0.2, 0.6) * T
+        a = (np.pi * 0.01 * (t - t1)) ** 2
+        obs[i] = (1 - 2 * a) * np.exp(-a)
+        a = (np.pi * 0.01 * (t - t1 - rng.normal(0, 3))) ** 2
+        sim[i] = (1 - 2 * a) * np.exp(-a) + rng.normal(0, 1e-3, T)
+    s = torch.as_tensor(sim).cuda()
+    o = torch.as_tensor(obs).cuda()
+    adj = torch.empty_like(s)
+    mis = torch.empty(n, dtype=torch.float64, device="cuda")
+    cpu = {"wasserstein": mo.wasserstein, "wasserstein_quad": mo.wasserstein_quad, "l2": mo.L2,
+           "quad_envelope": mo.quad_envelope, "wasserstein_pm": mo.wasserstein_pm,
+           "wasserstein_softplus": mo.wasserstein_softplus}
+    out = {}
+    for name, kind in MISFITS.items():
+        nb = int(L.otf_misfit_scratch_bytes(kind, n, T))
+        scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device="cuda")
+        st = torch.cuda.current_stream()
+
+        def call():
+            rc = L.otf_misfit(kind, ctypes.c_void_p(s.data_ptr()), ctypes.c_void_p(o.data_ptr()),
+                              ctypes.c_void_p(adj.data_ptr()), ctypes.c_void_p(mis.data_ptr()), n, T,
+                              ctypes.c_void_p(scratch.data_ptr()), nb, ctypes.c_void_p(st.cuda_stream))
+            if rc:
+                _lib.check(L)
+        for _ in range(args.warmup):
+            call()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            call()
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        rec = {"ms": round(ms, 3), "traces_per_s": round(n / (ms / 1e3), 1)}
+        if name in cpu:
+            k = 16
+            t0 = time.perf_counter()
+            cpu[name](sim[:k].astype(np.float64), obs[:k])
+            dt = time.perf_counter() - t0
+            rec["cpu_traces_per_s"] = round(k / dt, 1)
+            rec["speedup"] = round(rec["traces_per_s"] / rec["cpu_traces_per_s"], 1)
+        out[name] = rec
+    print(json.dumps({"metric": "device misfit traces/s", "leg": "misfits", "unit": "traces/s",
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+                      "config": {"workload": f"{n} traces x {T} samples"},
+                      "cpu_baseline": {"kind": "port", "cores": 1,
+                                       "sample": "oracle/misfit_oracle.py (the reference's numpy recipes), 16 traces"},
+                      "kinds": out}), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.leg == "cpml":
+        run_cpml_impl(args) if args.cpml_impl else run_cpml_leg(args)
+    elif args.leg == "misfits":
+        run_misfit_leg(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
