@@ -9,7 +9,8 @@
 // (halo recomputed, not exchanged), then the second derivatives, their
 // memory variables and P(t) = 2 P(t-1) - P(t-2) + lap dt^2 kappa on the
 // owned cells. Source injection (:210-231) and recording (:238-246) are two
-// small launches after it, as in the reference. Fields keep the reference's
+// small launches after it, as in the reference; the forward time loop is
+// replayed as one CUDA graph. Fields keep the reference's
 // layout: P in four time slots [4][Z][X] (so cells outside the update region
 // hold what the reference's would), memory variables of the first
 // derivatives in two slots (the halo recompute reads t-1 while owners write
@@ -146,10 +147,11 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
 // somaFonte (regression_CPML.cu:210-231): P += 4pi c^2 s(t) dt^2; with one
 // pixel per element only source idx fires (all when idx == -1), otherwise
 // every source fires.
-__global__ void k_cpml_source(float *Pn, int X, int T, int t, int ns, int ppe, int idx, const int *sx,
+__global__ void k_cpml_source(float *Pn, int X, int T, int t, int ns, int ppe, const int *idx_dev, const int *sx,
                               const int *sz, const float *cquad, const float *src, float qtpi, float dt2)
 {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int idx = *idx_dev;  // read on the device: one captured time loop serves every idx_source
     if (n >= ns || (ppe == 1 && idx != -1 && idx != n))
         return;
     const size_t i = (size_t)sz[n] * X + sx[n];
@@ -273,9 +275,20 @@ struct State {
     float *src = nullptr, *init = nullptr, *rec_d = nullptr, *rec_h = nullptr;
     int *sx = nullptr, *sz = nullptr, *pmx = nullptr, *pmz = nullptr;
     int cap_src = 0;
+    int *idx_dev = nullptr, *idx_h = nullptr;  // idx_source of the current call (device / pinned host)
+    // the forward time loop captured as a CUDA graph, for the source count it
+    // was captured with (set_source may change it)
+    cudaGraphExec_t sim_graph = nullptr;
+    int sim_graph_ns = -1;
 
     void release()
     {
+        if (sim_graph)
+            cudaGraphExecDestroy(sim_graph);
+        if (idx_dev)
+            cudaFree(idx_dev);
+        if (idx_h)
+            cudaFreeHost(idx_h);
         float *f[] = {P, mx, mz, mxx, mzz, cquad, kappa, rho_hx, rho_hz, cx, cz, src, init, rec_d};
         for (float *p : f)
             if (p)
@@ -356,6 +369,8 @@ static int init(int X, int Z, int T, int ns, int nm, int ppe, const int *ps_x, c
     OTF_CUDA(cudaMalloc(&g.src, (size_t)g.cap_src * T * sizeof(float)));
     OTF_CUDA(cudaMalloc(&g.sx, g.cap_src * sizeof(int)));
     OTF_CUDA(cudaMalloc(&g.sz, g.cap_src * sizeof(int)));
+    OTF_CUDA(cudaMalloc(&g.idx_dev, sizeof(int)));
+    OTF_CUDA(cudaMallocHost(&g.idx_h, sizeof(int)));
     OTF_CUDA(cudaMalloc(&g.pmx, std::max(nm, 1) * sizeof(int)));
     OTF_CUDA(cudaMalloc(&g.pmz, std::max(nm, 1) * sizeof(int)));
     OTF_CUDA(cudaMemcpy(g.cquad, cq, XZ * sizeof(float), cudaMemcpyHostToDevice));
@@ -424,8 +439,16 @@ static int reset_state()
     return 0;
 }
 
+// idx_source of the next launches, read by k_cpml_source from the device
+static int set_idx(int idx)
+{
+    *g.idx_h = idx;
+    OTF_CUDA(cudaMemcpyAsync(g.idx_dev, g.idx_h, sizeof(int), cudaMemcpyHostToDevice, g.st));
+    return 0;
+}
+
 // one time step t >= 2: the fused step and the source injection (lap optional)
-static void step(StepArgs &a, int t, int idx, float *lap)
+static void step(StepArgs &a, int t, float *lap)
 {
     const size_t XZ = (size_t)g.X * g.Z;
     float *Pn = g.P + (size_t)(t % 4) * XZ;
@@ -444,28 +467,60 @@ static void step(StepArgs &a, int t, int idx, float *lap)
     else
         k_cpml_step<true><<<grid, NTH, 0, g.st>>>(a);
     if (g.ns > 0)
-        k_cpml_source<<<(g.ns + 127) / 128, 128, 0, g.st>>>(Pn, g.X, g.T, t, g.ns, g.ppe, idx, g.sx, g.sz,
+        k_cpml_source<<<(g.ns + 127) / 128, 128, 0, g.st>>>(Pn, g.X, g.T, t, g.ns, g.ppe, g.idx_dev, g.sx, g.sz,
                                                            g.cquad, g.src, g.qtpi, g.dt2);
 }
 
-static int simulate(int idx)
+// the forward time loop: state reset, T-2 steps, the recording of every step
+static int emit_forward()
 {
-    OTF_CHECK(g.P != nullptr, 2, "cpml cuda_simulate2 called before init_memory_sim");
     const int X = g.X, T = g.T;
     const size_t XZ = (size_t)X * g.Z;
-    cudaStream_t st = g.st;
     if (reset_state())
         return -1;
     StepArgs a;
     fill_args(a);
     for (int t = 0; t < T; t++) {
         if (t > 1)
-            step(a, t, idx, nullptr);
+            step(a, t, nullptr);
         if (g.nm > 0)
-            k_cpml_record<<<(g.nm + 127) / 128, 128, 0, st>>>(g.P + (size_t)(t % 4) * XZ, X, T, t, g.nm, g.pmx,
-                                                              g.pmz, g.rec_d);
+            k_cpml_record<<<(g.nm + 127) / 128, 128, 0, g.st>>>(g.P + (size_t)(t % 4) * XZ, X, T, t, g.nm, g.pmx,
+                                                                g.pmz, g.rec_d);
     }
     OTF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// The forward loop is captured once (per source count) as a CUDA graph and
+// replayed: three small launches per step on a 2D field are launch-bound
+// when issued one by one.
+static int simulate(int idx)
+{
+    OTF_CHECK(g.P != nullptr, 2, "cpml cuda_simulate2 called before init_memory_sim");
+    const int T = g.T;
+    cudaStream_t st = g.st;
+    if (set_idx(idx))
+        return -1;
+    if (!g.sim_graph || g.sim_graph_ns != g.ns) {
+        if (g.sim_graph)
+            cudaGraphExecDestroy(g.sim_graph);
+        g.sim_graph = nullptr;
+        cudaGraph_t graph = nullptr;
+        OTF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int rc = emit_forward();
+        const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+        if (rc) {
+            if (graph)
+                cudaGraphDestroy(graph);
+            return -1;
+        }
+        OTF_CUDA(ec);
+        const cudaError_t ei = cudaGraphInstantiate(&g.sim_graph, graph, 0);
+        cudaGraphDestroy(graph);
+        OTF_CUDA(ei);
+        g.sim_graph_ns = g.ns;
+    }
+    OTF_CUDA(cudaGraphLaunch(g.sim_graph, st));
     if (g.nm > 0)
         OTF_CUDA(cudaMemcpyAsync(g.rec_h, g.rec_d, (size_t)g.nm * T * sizeof(float), cudaMemcpyDeviceToHost, st));
     OTF_CUDA(cudaStreamSynchronize(st));
@@ -501,7 +556,7 @@ static int gradient(int idx, int every, const float *g_h, float *grad_h)
     if (alloc((size_t)n_ck * 6 * XZ, &ck) || alloc((size_t)every * XZ, &lapb) || alloc(XZ, &LA) ||
         alloc(XZ, &LB) || alloc(XZ, &LC) || alloc(XZ, &lmx) || alloc(XZ, &lmz) || alloc(XZ, &lmxx) ||
         alloc(XZ, &lmzz) || alloc(XZ, &a0x) || alloc(XZ, &a0z) || alloc(XZ, &l0x) || alloc(XZ, &l0z) ||
-        alloc(XZ, &grad) || alloc(std::max<size_t>(1, (size_t)g.nm * T), &gd))
+        alloc(XZ, &grad) || alloc(std::max<size_t>(1, (size_t)g.nm * T), &gd) || set_idx(idx))
         return done(-1);
     auto save = [&](int j, int c) -> int {
         float *d = ck + (size_t)j * 6 * XZ;
@@ -525,7 +580,7 @@ static int gradient(int idx, int every, const float *g_h, float *grad_h)
     fill_args(a);
     for (int t = 1; t < T; t++) {
         if (t > 1)
-            step(a, t, idx, nullptr);
+            step(a, t, nullptr);
         if ((t - 1) % every == 0 && save((t - 1) / every, t))
             return done(-1);
     }
@@ -554,7 +609,7 @@ static int gradient(int idx, int every, const float *g_h, float *grad_h)
         if (restore(j, c))
             return done(-1);
         for (int t = c + 1; t <= end; t++)
-            step(a, t, idx, lapb + (size_t)(t - c - 1) * XZ);
+            step(a, t, lapb + (size_t)(t - c - 1) * XZ);
         for (int t = end; t > c; t--) {
             if (g.nm > 0)
                 k_cpml_adj_g<<<(g.nm + 127) / 128, 128, 0, st>>>(LA, gd, X, Z, T, t, g.nm, g.pmx, g.pmz);

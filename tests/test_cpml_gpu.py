@@ -59,6 +59,32 @@ def test_cpml_matches_reference_library_and_oracle(path):
     assert _rel(fast, o64) <= 1e-4
 
 
+def test_cpml_repeated_calls_replay_one_graph():
+    """The forward loop is one captured graph replayed with idx_source read on
+    the device: a sequence of calls with different sources (and a call after
+    set_source changes the source count) gives what fresh calls give."""
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r); sys.path.insert(0, %r);"
+        "import make_cpml_golden as m; sim, idx, ppe = m.case_sim('cpml_shot1', None);"
+        "a = [sim.simulate(i) for i in (1, -1, 0, 1)];"
+        "import ctypes; from ctypes import POINTER, c_int;"
+        "x = np.ascontiguousarray(sim.inputs['ps_x'][:2]); z = np.ascontiguousarray(sim.inputs['ps_z'][:2]);"
+        "sim.L.set_source(2, x.ctypes.data_as(POINTER(c_int)), z.ctypes.data_as(POINTER(c_int))); sim._check();"
+        "a.append(sim.simulate(-1)); np.save(sys.argv[1], np.stack(a))" % (ROOT, GOLDEN))
+    out = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"cpml_seq_{os.getpid()}.npy")
+    subprocess.run([sys.executable, "-c", code, out], check=True)
+    seq = np.load(out)
+    os.remove(out)
+    d = np.load(os.path.join(GOLDEN, "cpml_shot1.npz"))
+    X, Z, T, ppe = (int(d[k]) for k in ("X", "Z", "T", "ppe"))
+    inp = {k: d[k] for k in d.files}
+    assert np.array_equal(seq[0], d["traces"]) and np.array_equal(seq[3], d["traces"])
+    for i, idx in ((1, -1), (2, 0)):
+        assert np.array_equal(seq[i], co.simulate(inp, X, Z, T, idx_source=idx, ppe=ppe)), idx
+    two = dict(inp, ps_x=inp["ps_x"][:2], ps_z=inp["ps_z"][:2])
+    assert np.array_equal(seq[4], co.simulate(two, X, Z, T, idx_source=-1, ppe=ppe))
+
+
 def test_cpml_errors_are_reported():
     from otfwi_b200 import _lib
     from otfwi_b200.cpml import CPMLSimulator
