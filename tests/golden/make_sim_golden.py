@@ -14,7 +14,7 @@ file holds the inputs and the reference's outputs:
                             from the true model, at the start model
   sim_s<k>                  the traces the reference handed to the callback
 
-    python tests/golden/make_sim_golden.py --out gpurun_out/golden
+    python tests/golden/make_sim_golden.py --out /tmp/golden
 """
 import argparse
 import ctypes
