@@ -8,9 +8,9 @@
 // memory variables and the density division on the tile plus a 4-cell halo
 // (halo recomputed, not exchanged), then the second derivatives, their
 // memory variables and P(t) = 2 P(t-1) - P(t-2) + lap dt^2 kappa on the
-// owned cells. Source injection (:210-231) and recording (:238-246) are two
-// small launches after it, as in the reference; the forward time loop is
-// replayed as one CUDA graph. Fields keep the reference's
+// owned cells; the CTA then adds the sources (:210-231) and records the
+// receivers (:238-246) that lie in its tile, so a step is one launch (the
+// reference's are four). The forward time loop is replayed as one CUDA graph. Fields keep the reference's
 // layout: P in four time slots [4][Z][X] (so cells outside the update region
 // hold what the reference's would), memory variables of the first
 // derivatives in two slots (the halo recompute reads t-1 while owners write
@@ -53,6 +53,13 @@ struct StepArgs {
     float *mxx, *mzz;      // in place
     float *lap;            // optional: lap(t) of every owned cell (adjoint recompute)
     Coef c;
+    // point work of the step, done by the CTA owning the cell after its
+    // P(t): sources (somaFonte) then, when rec is set, the receivers
+    int T, ns, nm, ppe;
+    const int *idx_dev, *sx, *sz, *pmx, *pmz;
+    const float *cquad, *src;
+    float qtpi;
+    float *rec;
 };
 
 __device__ __forceinline__ bool inb(int X, int Z, int x, int z) { return x >= 4 && z >= 4 && x < X - 4 && z < Z - 4; }
@@ -142,21 +149,36 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
         if (a.lap)
             a.lap[i] = lap;
     }
-}
-
-// somaFonte (regression_CPML.cu:210-231): P += 4pi c^2 s(t) dt^2; with one
-// pixel per element only source idx fires (all when idx == -1), otherwise
-// every source fires.
-__global__ void k_cpml_source(float *Pn, int X, int T, int t, int ns, int ppe, const int *idx_dev, const int *sx,
-                              const int *sz, const float *cquad, const float *src, float qtpi, float dt2)
-{
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    const int idx = *idx_dev;  // read on the device: one captured time loop serves every idx_source
-    if (n >= ns || (ppe == 1 && idx != -1 && idx != n))
+    if (a.ns == 0 && !a.rec)
         return;
-    const size_t i = (size_t)sz[n] * X + sx[n];
-    const float s = __fmul_rn(__fmul_rn(qtpi, cquad[i]), src[(size_t)n * T + t]);
-    Pn[i] = __fmaf_rn(s, dt2, Pn[i]);
+    // sources in this tile (somaFonte, regression_CPML.cu:210-231), then the
+    // receivers in it (:238-246), by the first warp: lanes test 32 points at
+    // a time, lane 0 applies the sources in source order (as a sequential
+    // loop would) and __syncwarp orders them before the recording reads
+    __syncthreads();
+    if (threadIdx.x >= 32)
+        return;
+    const int lane = threadIdx.x;
+    auto mine = [&](int px, int pz) { return px >= x0 && px < x0 + TX && pz >= z0 && pz < z0 + TZ; };
+    const int idx = a.ns > 0 ? *a.idx_dev : -1;
+    for (int base = 0; base < a.ns; base += 32) {
+        const int n = base + lane;
+        const bool hit = n < a.ns && !(a.ppe == 1 && idx != -1 && idx != n) && mine(a.sx[n], a.sz[n]);
+        unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0)
+            while (m) {
+                const int k = base + __ffs(m) - 1;
+                m &= m - 1;
+                const size_t i = (size_t)a.sz[k] * X + a.sx[k];
+                const float sv = __fmul_rn(__fmul_rn(a.qtpi, a.cquad[i]), a.src[(size_t)k * a.T + a.t]);
+                a.Pn[i] = __fmaf_rn(sv, a.c.dt2, a.Pn[i]);
+            }
+        __syncwarp();
+    }
+    if (a.rec)
+        for (int n = lane; n < a.nm; n += 32)
+            if (mine(a.pmx[n], a.pmz[n]))
+                a.rec[(size_t)n * a.T + a.t] = a.Pn[(size_t)a.pmz[n] * X + a.pmx[n]];
 }
 
 // gravaBufferSensores2ordem (regression_CPML.cu:238-246)
@@ -280,9 +302,13 @@ struct State {
     // was captured with (set_source may change it)
     cudaGraphExec_t sim_graph = nullptr;
     int sim_graph_ns = -1;
+    float *gbuf = nullptr;  // gradient work buffers, kept between calls
+    size_t gbuf_floats = 0;
 
     void release()
     {
+        if (gbuf)
+            cudaFree(gbuf);
         if (sim_graph)
             cudaGraphExecDestroy(sim_graph);
         if (idx_dev)
@@ -423,6 +449,19 @@ static void fill_args(StepArgs &a)
     a.mxx = g.mxx;
     a.mzz = g.mzz;
     a.lap = nullptr;
+    a.T = g.T;
+    a.ns = g.ns;
+    a.nm = g.nm;
+    a.ppe = g.ppe;
+    a.idx_dev = g.idx_dev;
+    a.sx = g.sx;
+    a.sz = g.sz;
+    a.pmx = g.pmx;
+    a.pmz = g.pmz;
+    a.cquad = g.cquad;
+    a.src = g.src;
+    a.qtpi = g.qtpi;
+    a.rec = nullptr;
 }
 
 // P(0), P(1) from the initial field, every other slot and memory variable zero
@@ -439,7 +478,7 @@ static int reset_state()
     return 0;
 }
 
-// idx_source of the next launches, read by k_cpml_source from the device
+// idx_source of the next launches, read by the step kernel from the device
 static int set_idx(int idx)
 {
     *g.idx_h = idx;
@@ -447,8 +486,9 @@ static int set_idx(int idx)
     return 0;
 }
 
-// one time step t >= 2: the fused step and the source injection (lap optional)
-static void step(StepArgs &a, int t, float *lap)
+// one time step t >= 2: one launch computes P(t), adds the sources and, with
+// rec, records the receivers (lap optional)
+static void step(StepArgs &a, int t, float *lap, float *rec = nullptr)
 {
     const size_t XZ = (size_t)g.X * g.Z;
     float *Pn = g.P + (size_t)(t % 4) * XZ;
@@ -461,14 +501,12 @@ static void step(StepArgs &a, int t, float *lap)
     a.mx_out = g.mx + (size_t)(t % 2) * XZ;
     a.mz_out = g.mz + (size_t)(t % 2) * XZ;
     a.lap = lap;
+    a.rec = rec;
     const dim3 grid((g.X + TX - 1) / TX, (g.Z + TZ - 1) / TZ);
     if (g.precision == 1)
         k_cpml_step<false><<<grid, NTH, 0, g.st>>>(a);
     else
         k_cpml_step<true><<<grid, NTH, 0, g.st>>>(a);
-    if (g.ns > 0)
-        k_cpml_source<<<(g.ns + 127) / 128, 128, 0, g.st>>>(Pn, g.X, g.T, t, g.ns, g.ppe, g.idx_dev, g.sx, g.sz,
-                                                           g.cquad, g.src, g.qtpi, g.dt2);
 }
 
 // the forward time loop: state reset, T-2 steps, the recording of every step
@@ -482,8 +520,8 @@ static int emit_forward()
     fill_args(a);
     for (int t = 0; t < T; t++) {
         if (t > 1)
-            step(a, t, nullptr);
-        if (g.nm > 0)
+            step(a, t, nullptr, g.nm > 0 ? g.rec_d : nullptr);
+        else if (g.nm > 0)  // the initial field
             k_cpml_record<<<(g.nm + 127) / 128, 128, 0, g.st>>>(g.P + (size_t)(t % 4) * XZ, X, T, t, g.nm, g.pmx,
                                                                 g.pmz, g.rec_d);
     }
@@ -541,23 +579,32 @@ static int gradient(int idx, int every, const float *g_h, float *grad_h)
     const size_t XZ = (size_t)X * Z;
     cudaStream_t st = g.st;
     const int n_ck = (T - 2 + every - 1) / every + 1;  // checkpoints at 1 + j*every <= T-1
-    std::vector<float *> bufs;
-    auto alloc = [&](size_t n, float **p) -> int {
-        OTF_CUDA(cudaMalloc(p, n * sizeof(float)));
-        bufs.push_back(*p);
-        return 0;
+    // work buffers carved from one allocation kept between calls (grown when
+    // a call needs more): a per-call cudaMalloc / cudaFree of the checkpoints
+    // costs more than the adjoint itself on small grids
+    const size_t n_trace = std::max<size_t>(1, (size_t)g.nm * T);
+    const size_t need = (size_t)n_ck * 6 * XZ + (size_t)every * XZ + 13 * XZ + n_trace;
+    if (need > g.gbuf_floats) {
+        if (g.gbuf)
+            cudaFree(g.gbuf);
+        g.gbuf = nullptr;
+        g.gbuf_floats = 0;
+        OTF_CUDA(cudaMalloc(&g.gbuf, need * sizeof(float)));
+        g.gbuf_floats = need;
+    }
+    auto done = [&](int rc) { return rc; };
+    float *cur = g.gbuf;
+    auto carve = [&](size_t n) {
+        float *p = cur;
+        cur += n;
+        return p;
     };
-    auto done = [&](int rc) {
-        for (float *p : bufs)
-            cudaFree(p);
-        return rc;
-    };
-    float *ck, *lapb, *LA, *LB, *LC, *lmx, *lmz, *lmxx, *lmzz, *a0x, *a0z, *l0x, *l0z, *grad, *gd;
-    if (alloc((size_t)n_ck * 6 * XZ, &ck) || alloc((size_t)every * XZ, &lapb) || alloc(XZ, &LA) ||
-        alloc(XZ, &LB) || alloc(XZ, &LC) || alloc(XZ, &lmx) || alloc(XZ, &lmz) || alloc(XZ, &lmxx) ||
-        alloc(XZ, &lmzz) || alloc(XZ, &a0x) || alloc(XZ, &a0z) || alloc(XZ, &l0x) || alloc(XZ, &l0z) ||
-        alloc(XZ, &grad) || alloc(std::max<size_t>(1, (size_t)g.nm * T), &gd) || set_idx(idx))
-        return done(-1);
+    float *ck = carve((size_t)n_ck * 6 * XZ), *lapb = carve((size_t)every * XZ);
+    float *LA = carve(XZ), *LB = carve(XZ), *LC = carve(XZ), *lmx = carve(XZ), *lmz = carve(XZ);
+    float *lmxx = carve(XZ), *lmzz = carve(XZ), *a0x = carve(XZ), *a0z = carve(XZ), *l0x = carve(XZ);
+    float *l0z = carve(XZ), *grad = carve(XZ), *gd = carve(n_trace);
+    if (set_idx(idx))
+        return -1;
     auto save = [&](int j, int c) -> int {
         float *d = ck + (size_t)j * 6 * XZ;
         const float *src[6] = {g.P + (size_t)(c % 4) * XZ, g.P + (size_t)((c + 3) % 4) * XZ,
