@@ -77,10 +77,11 @@ class CPMLSimulator:
     1); src_mask / rec_mask: boolean [Z, X]; source: waveforms [n_src, T];
     dx, dt: spacing and step (the CFL number c dt / dx must stay below about
     0.55 for this stencil); ppe: pixels per element (1: ``simulate(idx)``
-    fires source idx alone). ``lib``: path of a library with the CPML ABI."""
+    fires source idx alone); k_max: the CPML stretching K at the outer edge.
+    ``lib``: path of a library with the CPML ABI."""
 
     def __init__(self, X, Z, T, PML, c, src_mask, rec_mask, source, rho=None, dx=1.0, dt=1.0, f0=0.05,
-                 qtpi=4.0 * np.pi, ppe=1, init=None, lib=None):
+                 qtpi=4.0 * np.pi, ppe=1, init=None, lib=None, k_max=1.0):
         self.lib_path = lib or CPML_LIB
         self.L = _declare(ctypes.CDLL(os.path.abspath(self.lib_path)))
         self.X, self.Z, self.T = X, Z, T
@@ -94,8 +95,8 @@ class CPMLSimulator:
         rhx[:, :-1] = 0.5 * (rho[:, :-1] + rho[:, 1:])
         rhz = rho.copy()
         rhz[:-1, :] = 0.5 * (rho[:-1, :] + rho[1:, :])
-        (px, pxh) = cpml_profiles(X, PML, dx, dt, float(c.max()), f0)
-        (pz, pzh) = cpml_profiles(Z, PML, dx, dt, float(c.max()), f0)
+        (px, pxh) = cpml_profiles(X, PML, dx, dt, float(c.max()), f0, k_max=k_max)
+        (pz, pzh) = cpml_profiles(Z, PML, dx, dt, float(c.max()), f0, k_max=k_max)
         f32 = lambda a: np.ascontiguousarray(np.asarray(a, np.float32).ravel())
         i32 = lambda a: np.ascontiguousarray(np.asarray(a, np.int32).ravel())
         self._keep = keep = {

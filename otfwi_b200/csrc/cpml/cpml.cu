@@ -21,6 +21,7 @@
 // with the contractions fma(b, m, a*v) and fma(lap*dt2, kappa, 2 P1 - P2),
 // IEEE divisions; fast uses the FP32 antisymmetric-pair staggered sums.
 #include <cuda_runtime.h>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -42,7 +43,18 @@ struct Coef {
     const float *Kz, *az, *bz, *Kzh, *azh, *bzh;  // [Z]
     const float *kappa, *rho_hx, *rho_hz;         // [Z][X]
     float dx, dz, dt2;
+    // Divisions the step may skip without changing a bit: by a power-of-two
+    // spacing (multiplication by its exact reciprocal rounds the same) and by
+    // a K profile that is 1 everywhere (k_max = 1, the usual CPML).
+    float inv_dx, inv_dz;  // 0 when the spacing is not a power of two
+    int k_one;             // bit 0 Kx, 1 Kxh, 2 Kz, 3 Kzh all exactly 1
 };
+
+// v / d, IEEE-rounded, as a product when d is a power of two (inv != 0)
+__device__ __forceinline__ float div_sp(float v, float d, float inv)
+{
+    return inv != 0.f ? __fmul_rn(v, inv) : __fdiv_rn(v, d);
+}
 
 struct StepArgs {
     int X, Z, t;
@@ -113,12 +125,14 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
         if (inb(X, Z, x, z)) {
             const size_t i = (size_t)z * X + x;
             // offset 0: taps x-3 .. x+4 (tile column of x is ex + 4)
-            const float v0x = __fdiv_rn(stag<FAITHFUL>(&sP[ez + 4][ex + 1], 1), a.c.dx);
+            const float v0x = div_sp(stag<FAITHFUL>(&sP[ez + 4][ex + 1], 1), a.c.dx, a.c.inv_dx);
             const float mx = __fmaf_rn(a.c.bxh[x], a.mx_in[i], __fmul_rn(a.c.axh[x], v0x));
-            vx = __fdiv_rn(__fadd_rn(__fdiv_rn(v0x, a.c.Kxh[x]), mx), a.c.rho_hx[i]);
-            const float v0z = __fdiv_rn(stag<FAITHFUL>(&sP[ez + 1][ex + 4], SW), a.c.dz);
+            const float kx = (a.c.k_one & 2) ? v0x : __fdiv_rn(v0x, a.c.Kxh[x]);
+            vx = __fdiv_rn(__fadd_rn(kx, mx), a.c.rho_hx[i]);
+            const float v0z = div_sp(stag<FAITHFUL>(&sP[ez + 1][ex + 4], SW), a.c.dz, a.c.inv_dz);
             const float mz = __fmaf_rn(a.c.bzh[z], a.mz_in[i], __fmul_rn(a.c.azh[z], v0z));
-            vz = __fdiv_rn(__fadd_rn(__fdiv_rn(v0z, a.c.Kzh[z]), mz), a.c.rho_hz[i]);
+            const float kz = (a.c.k_one & 8) ? v0z : __fdiv_rn(v0z, a.c.Kzh[z]);
+            vz = __fdiv_rn(__fadd_rn(kz, mz), a.c.rho_hz[i]);
             if (ex >= 4 && ex < TX + 4 && ez >= 4 && ez < TZ + 4) {
                 a.mx_out[i] = mx;
                 a.mz_out[i] = mz;
@@ -136,14 +150,14 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
             continue;
         const size_t i = (size_t)z * X + x;
         // offset 1: taps x-4 .. x+3 (region column of x is ox + 4)
-        const float vxx0 = __fdiv_rn(stag<FAITHFUL>(&sVx[oz + 4][ox], 1), a.c.dx);
+        const float vxx0 = div_sp(stag<FAITHFUL>(&sVx[oz + 4][ox], 1), a.c.dx, a.c.inv_dx);
         const float mxx = __fmaf_rn(a.c.bx[x], a.mxx[i], __fmul_rn(a.c.ax[x], vxx0));
         a.mxx[i] = mxx;
-        const float vxx1 = __fadd_rn(__fdiv_rn(vxx0, a.c.Kx[x]), mxx);
-        const float vzz0 = __fdiv_rn(stag<FAITHFUL>(&sVz[oz][ox + 4], VW), a.c.dz);
+        const float vxx1 = __fadd_rn((a.c.k_one & 1) ? vxx0 : __fdiv_rn(vxx0, a.c.Kx[x]), mxx);
+        const float vzz0 = div_sp(stag<FAITHFUL>(&sVz[oz][ox + 4], VW), a.c.dz, a.c.inv_dz);
         const float mzz = __fmaf_rn(a.c.bz[z], a.mzz[i], __fmul_rn(a.c.az[z], vzz0));
         a.mzz[i] = mzz;
-        const float vzz1 = __fadd_rn(__fdiv_rn(vzz0, a.c.Kz[z]), mzz);
+        const float vzz1 = __fadd_rn((a.c.k_one & 4) ? vzz0 : __fdiv_rn(vzz0, a.c.Kz[z]), mzz);
         const float lap = __fadd_rn(vxx1, vzz1);
         a.Pn[i] = __fmaf_rn(__fmul_rn(lap, a.c.dt2), a.c.kappa[i], __fmaf_rn(2.f, a.P1[i], -a.P2[i]));
         if (a.lap)
@@ -302,6 +316,8 @@ struct State {
     // was captured with (set_source may change it)
     cudaGraphExec_t sim_graph = nullptr;
     int sim_graph_ns = -1;
+    float inv_dx = 0.f, inv_dz = 0.f;  // exact reciprocals of power-of-two spacings, else 0
+    int k_one = 0;                     // K profiles that are exactly 1 (bits Kx, Kxh, Kz, Kzh)
     float *gbuf = nullptr;  // gradient work buffers, kept between calls
     size_t gbuf_floats = 0;
 
@@ -416,6 +432,22 @@ static int init(int X, int Z, int T, int ns, int nm, int ppe, const int *ps_x, c
         OTF_CUDA(cudaMemcpy(g.pmx, pm_x, nm * sizeof(int), cudaMemcpyHostToDevice));
         OTF_CUDA(cudaMemcpy(g.pmz, pm_z, nm * sizeof(int), cudaMemcpyHostToDevice));
     }
+    // divisions the step may replace exactly (see Coef)
+    auto pow2_inv = [](float d) {
+        int e = 0;
+        const float m = std::frexp(d, &e);
+        return (d > 0.f && m == 0.5f) ? std::ldexp(1.f, 1 - e) : 0.f;
+    };
+    g.inv_dx = pow2_inv(dx);
+    g.inv_dz = pow2_inv(dz);
+    auto all_one = [](const float *v, int n) {
+        for (int k = 0; k < n; k++)
+            if (v[k] != 1.f)
+                return false;
+        return true;
+    };
+    g.k_one = (all_one(cx6[0], X) ? 1 : 0) | (all_one(cx6[3], X) ? 2 : 0) | (all_one(cz6[0], Z) ? 4 : 0) |
+              (all_one(cz6[3], Z) ? 8 : 0);
     if (init_h)
         OTF_CUDA(cudaMemcpy(g.init, init_h, 2 * XZ * sizeof(float), cudaMemcpyHostToDevice));
     else
@@ -445,6 +477,9 @@ static void fill_args(StepArgs &a)
     a.c.rho_hz = g.rho_hz;
     a.c.dx = g.dx;
     a.c.dz = g.dz;
+    a.c.inv_dx = g.inv_dx;
+    a.c.inv_dz = g.inv_dz;
+    a.c.k_one = g.k_one;
     a.c.dt2 = g.dt2;
     a.mxx = g.mxx;
     a.mzz = g.mzz;

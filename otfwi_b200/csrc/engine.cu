@@ -2,6 +2,7 @@
 // of the time loops, and the small helper kernels around the fused steps.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -964,6 +965,30 @@ int Engine::variant_in_use() const
     return resolve_variant(k, variant_ >= 3 ? 2 : variant_, cfg_.precision);
 }
 
+// Launch with programmatic stream serialization (programmatic dependent
+// launch): the kernel may begin launching while its predecessor drains; the
+// kernels synchronise on the predecessor themselves (pdl_enter). OTFWI_PDL=0
+// launches them plainly.
+template <class... A>
+static cudaError_t launch_pdl(void (*kernel)(A...), dim3 grid, dim3 block, cudaStream_t st, A... args)
+{
+    static const bool use = [] {
+        const char *v = getenv("OTFWI_PDL");
+        return !(v && v[0] == '0');
+    }();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = use ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Unfused half-step launches (pml_step_unfused.cuh): forward P then A (with
 // the receiver / ring recording CTAs); reverse P of both sets, the ring
 // overwrite, then A of both sets with the imaging condition.
@@ -986,19 +1011,21 @@ int Engine::launch_unfused(const StepParams &p, int kind)
     U.record_ring = kind == 1;
     const dim3 grid(U.ncb, U.nseg, n_shots_);
     if (kind < 2) {
-        k_unfused_p_fwd<<<grid, kUThreads, 0, st_>>>(U);
+        OTF_CUDA(launch_pdl(k_unfused_p_fwd, grid, dim3(kUThreads), st_, U));
         if (U.n_src_cells > 0)
-            k_unfused_points<false><<<dim3((U.n_src_cells + 127) / 128, n_shots_), 128, 0, st_>>>(U);
+            OTF_CUDA(launch_pdl(k_unfused_points<false>, dim3((U.n_src_cells + 127) / 128, n_shots_), dim3(128),
+                                st_, U));
         const int extra = n_rec_ + (kind == 1 ? n_ring_ : 0);
         const int per_row = U.ncb * kUThreads * kUTailPer;
         const int tail = (extra + per_row - 1) / per_row;
-        k_unfused_a_fwd<<<dim3(U.ncb, U.nseg + tail, n_shots_), kUThreads, 0, st_>>>(U);
+        OTF_CUDA(launch_pdl(k_unfused_a_fwd, dim3(U.ncb, U.nseg + tail, n_shots_), dim3(kUThreads), st_, U));
     } else {
-        k_unfused_p_rev<<<dim3(U.ncb, U.nseg, 2 * n_shots_), kUThreads, 0, st_>>>(U, n_shots_);
+        OTF_CUDA(launch_pdl(k_unfused_p_rev, dim3(U.ncb, U.nseg, 2 * n_shots_), dim3(kUThreads), st_, U,
+                            n_shots_));
         const int np = n_ring_ + U.n_rcv_cells;
         if (np > 0)
-            k_unfused_points<true><<<dim3((np + 127) / 128, n_shots_), 128, 0, st_>>>(U);
-        k_unfused_a_rev<<<grid, kUThreads, 0, st_>>>(U);
+            OTF_CUDA(launch_pdl(k_unfused_points<true>, dim3((np + 127) / 128, n_shots_), dim3(128), st_, U));
+        OTF_CUDA(launch_pdl(k_unfused_a_rev, grid, dim3(kUThreads), st_, U));
     }
     OTF_CUDA(cudaGetLastError());
     return 0;

@@ -60,6 +60,21 @@ struct UnfusedParams {
     int record_ring;  // forward: also record the boundary ring
 };
 
+// Programmatic dependent launch: the engine launches these kernels with
+// programmatic stream serialization, so a kernel's CTAs may be scheduled
+// while its predecessor's last CTAs still run (hiding the launch gap and the
+// predecessor's tail). Every kernel waits here, before touching memory,
+// until the predecessor grid has completed and its writes are visible, then
+// allows its own successor to start launching. Without the launch attribute
+// both calls return at once.
+__device__ __forceinline__ void pdl_enter()
+{
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+#endif
+}
+
 __device__ __forceinline__ float4 uld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
 __device__ __forceinline__ float4 uld4c(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void ust4(float *p, const float *v)
@@ -163,6 +178,7 @@ constexpr int kUAMinBlocks = 28;
 // Forward P half-step: grid (ncb, nseg, n_shots).
 __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const __grid_constant__ UnfusedParams U)
 {
+    pdl_enter();
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= U.p.X)
         return;
@@ -173,6 +189,7 @@ __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const
 // n_shots: reconstruction (set 0, q0), else adjoint (set 1, q1).
 __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_rev(const __grid_constant__ UnfusedParams U, int n_shots)
 {
+    pdl_enter();
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= U.p.X)
         return;
@@ -208,6 +225,7 @@ __device__ __forceinline__ void a_update(const StepParams &p, bool revert, float
 // that these latency-bound CTAs run beside the stencil CTAs, not after them.
 __global__ void __launch_bounds__(kUThreads, kUAMinBlocks) k_unfused_a_fwd(const __grid_constant__ UnfusedParams U)
 {
+    pdl_enter();
     const StepParams &p = U.p;
     const int shot = blockIdx.z;
     const int64_t so = p.shot_stride * shot;
@@ -289,6 +307,7 @@ __global__ void __launch_bounds__(kUThreads, kUAMinBlocks) k_unfused_a_fwd(const
 // nseg, n_shots).
 __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_constant__ UnfusedParams U)
 {
+    pdl_enter();
     const StepParams &p = U.p;
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= p.X)
@@ -424,6 +443,7 @@ __device__ __forceinline__ void inject_cell(const StepParams &p, const Fields &f
 template <bool RING>
 __global__ void __launch_bounds__(128) k_unfused_points(const __grid_constant__ UnfusedParams U)
 {
+    pdl_enter();
     const StepParams &p = U.p;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int shot = blockIdx.y;
