@@ -275,8 +275,8 @@ def run_ours(args):
     ach_fwd = BYTES_FWD * per_launch_cells / (ms_fwd / 1e3) / 1e9
     tr = profile_traffic(args.kernel)
     if args.kernel == 4:
-        rev_name = ("reverse step (k_unfused_p_rev + k_unfused_points<1> + k_unfused_a_rev: adjoint + "
-                    "reconstruction + imaging condition, all shots; 88 B/cell moved)")
+        rev_name = ("reverse step (k_unfused_p_rev + k_unfused_a_rev: adjoint + reconstruction + "
+                    "imaging condition, all shots; 88 B/cell moved)")
     else:
         rev_name = "k_reverse_split (adjoint + reconstruction + imaging condition, all shots)"
     roof = {"kernel": rev_name,
@@ -347,9 +347,9 @@ def run_ours(args):
                                stream_rows=args.stream_rows if args.kernel == 3 else None),
                 "roofline": roof, "e2e": e2e,
                 # per time step one fused launch forward and one reverse (the
-                # unfused variant 4: P, point and A launches in each); per
+                # unfused variant 4: a P and an A launch in each); per
                 # gradient the misfit, its sum, the running integral, shot mean
-                "gpu_launches": args.steps * ((6 if args.kernel == 4 else 2) * (sc.T - 1) + 4),
+                "gpu_launches": args.steps * ((4 if args.kernel == 4 else 2) * (sc.T - 1) + 4),
                 "clocks": clk.summary(),
                 "misfit_value": float(mis.item())}
         if not args.no_cpu_baseline:

@@ -1,6 +1,7 @@
 // Engine implementation: device buffers, per-tile point tables, CUDA graphs
 // of the time loops, and the small helper kernels around the fused steps.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -771,38 +772,64 @@ int Engine::build_tables()
         h.push_back(0);
     }
     // unfused kernels: distinct injection cells (padded offset) with their
-    // source / receiver indices in increasing order (CSR); padded offsets of
-    // receivers and ring cells
-    const int NCB = (X + kUCols - 1) / kUCols, NSEG = (Z + kURows - 1) / kURows;
+    // source / receiver indices in increasing order (CSR), the cells grouped
+    // by the P-kernel CTA (column block cb, row segment sg; key cb + NCB *
+    // sg) that owns them; the ring cells grouped the same way; padded
+    // offsets of receivers and ring cells
+    const int NCB = (X + kUCols - 1) / kUCols, NSEG = (Z + kURows - 1) / kURows, NC = NCB * NSEG;
+    auto cta_of = [&](int x, int z) { return (z / kURows) * NCB + x / kUCols; };
     size_t o_usrc = 0, o_urcv = 0;
     int n_ucells[2] = {0, 0};
     for (int pass = 0; pass < 2; pass++) {
-        std::vector<std::pair<int, int>> pts;  // (offset, index)
+        std::vector<std::array<int, 4>> pts;  // (cta, offset, index)
         if (pass == 0)
             for (int k = 0; k < n_src_; k++)
-                pts.push_back({(int)L_.at(src_x_[k], src_z_[k]), k});
+                pts.push_back({cta_of(src_x_[k], src_z_[k]), (int)L_.at(src_x_[k], src_z_[k]), k, 0});
         else
             for (int n = 0; n < n_rec_; n++)
                 if (interior(rec_x_[n], rec_z_[n], X, Z))
-                    pts.push_back({(int)L_.at(rec_x_[n], rec_z_[n]), n});
-        std::stable_sort(pts.begin(), pts.end());
-        std::vector<int> ptr(1, 0), off, id;
+                    pts.push_back({cta_of(rec_x_[n], rec_z_[n]), (int)L_.at(rec_x_[n], rec_z_[n]), n, 0});
+        std::sort(pts.begin(), pts.end());
+        std::vector<int> ptr(1, 0), off, id, cta(NC + 1, 0);
         for (size_t e = 0; e < pts.size(); e++) {
-            if (e == 0 || pts[e].first != pts[e - 1].first) {
-                off.push_back(pts[e].first);
+            if (e == 0 || pts[e][1] != pts[e - 1][1]) {
+                off.push_back(pts[e][1]);
+                cta[pts[e][0] + 1]++;
                 if (e > 0)
                     ptr.push_back((int)e);
             }
-            id.push_back(pts[e].second);
+            id.push_back(pts[e][2]);
         }
         if (!pts.empty())
             ptr.push_back((int)pts.size());
+        for (int c = 0; c < NC; c++)
+            cta[c + 1] += cta[c];
         n_ucells[pass] = (int)off.size();
         (pass ? o_urcv : o_usrc) = h.size();
         h.insert(h.end(), ptr.begin(), ptr.end());
         h.insert(h.end(), off.begin(), off.end());
         h.push_back(0);
         h.insert(h.end(), id.begin(), id.end());
+        h.push_back(0);
+        h.insert(h.end(), cta.begin(), cta.end());
+    }
+    const size_t o_uring = h.size();
+    {
+        std::vector<std::array<int, 3>> rc;  // (cta, offset, ring index)
+        for (int n = 0; n < n_ring_; n++)
+            rc.push_back({cta_of(ring_x_[n], ring_z_[n]), (int)L_.at(ring_x_[n], ring_z_[n]), n});
+        std::sort(rc.begin(), rc.end());
+        std::vector<int> cta(NC + 1, 0);
+        for (auto &e : rc)
+            cta[e[0] + 1]++;
+        for (int c = 0; c < NC; c++)
+            cta[c + 1] += cta[c];
+        h.insert(h.end(), cta.begin(), cta.end());
+        for (auto &e : rc)
+            h.push_back(e[1]);
+        h.push_back(0);
+        for (auto &e : rc)
+            h.push_back(e[2]);
         h.push_back(0);
     }
     const size_t o_uoff = h.size();
@@ -879,12 +906,25 @@ int Engine::build_tables()
     stb_.strip_edge = d + o_sedge;
     n_strips_ = NS;
     // CSR blocks: ptr [cells + 1] (just [0] when empty), off [cells] + 1, id + 1
-    utb_.src_ptr = d + o_usrc;
-    utb_.src_off = utb_.src_ptr + n_ucells[0] + 1;
-    utb_.src_id = utb_.src_off + n_ucells[0] + 1;
-    utb_.rcv_ptr = d + o_urcv;
-    utb_.rcv_off = utb_.rcv_ptr + n_ucells[1] + 1;
-    utb_.rcv_id = utb_.rcv_off + n_ucells[1] + 1;
+    {
+        // per block: ptr [cells + 1], off [cells] + 1, id [points] + 1, cta [NC + 1]
+        int n_pts[2] = {0, 0};
+        for (int k = 0; k < n_src_; k++)
+            n_pts[0]++;
+        for (int n = 0; n < n_rec_; n++)
+            n_pts[1] += interior(rec_x_[n], rec_z_[n], X, Z) ? 1 : 0;
+        utb_.src_ptr = d + o_usrc;
+        utb_.src_off = utb_.src_ptr + n_ucells[0] + 1;
+        utb_.src_id = utb_.src_off + n_ucells[0] + 1;
+        utb_.src_cta = utb_.src_id + n_pts[0] + 1;
+        utb_.rcv_ptr = d + o_urcv;
+        utb_.rcv_off = utb_.rcv_ptr + n_ucells[1] + 1;
+        utb_.rcv_id = utb_.rcv_off + n_ucells[1] + 1;
+        utb_.rcv_cta = utb_.rcv_id + n_pts[1] + 1;
+        utb_.ring_cta = d + o_uring;
+        utb_.ring_cta_off = utb_.ring_cta + NC + 1;
+        utb_.ring_cta_k = utb_.ring_cta_off + n_ring_ + 1;
+    }
     utb_.n_src_cells = n_ucells[0];
     utb_.n_rcv_cells = n_ucells[1];
     utb_.rec_off = d + o_uoff;
@@ -989,9 +1029,10 @@ static cudaError_t launch_pdl(void (*kernel)(A...), dim3 grid, dim3 block, cudaS
     return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-// Unfused half-step launches (pml_step_unfused.cuh): forward P then A (with
-// the receiver / ring recording CTAs); reverse P of both sets, the ring
-// overwrite, then A of both sets with the imaging condition.
+// Unfused half-step launches (pml_step_unfused.cuh): forward P (with the
+// sources) then A (with the receiver / ring recording CTAs); reverse P of
+// both sets (with the ring overwrite and the adjoint sources), then A of
+// both sets with the imaging condition.
 int Engine::launch_unfused(const StepParams &p, int kind)
 {
     UnfusedParams U;
@@ -1006,15 +1047,17 @@ int Engine::launch_unfused(const StepParams &p, int kind)
     U.rcv_off = utb_.rcv_off;
     U.rcv_id = utb_.rcv_id;
     U.n_rcv_cells = utb_.n_rcv_cells;
+    U.src_cta = utb_.src_cta;
+    U.rcv_cta = utb_.rcv_cta;
+    U.ring_cta = utb_.ring_cta;
+    U.ring_cta_off = utb_.ring_cta_off;
+    U.ring_cta_k = utb_.ring_cta_k;
     U.rec_off = utb_.rec_off;
     U.ring_off = utb_.ring_off;
     U.record_ring = kind == 1;
     const dim3 grid(U.ncb, U.nseg, n_shots_);
     if (kind < 2) {
         OTF_CUDA(launch_pdl(k_unfused_p_fwd, grid, dim3(kUThreads), st_, U));
-        if (U.n_src_cells > 0)
-            OTF_CUDA(launch_pdl(k_unfused_points<false>, dim3((U.n_src_cells + 127) / 128, n_shots_), dim3(128),
-                                st_, U));
         const int extra = n_rec_ + (kind == 1 ? n_ring_ : 0);
         const int per_row = U.ncb * kUThreads * kUTailPer;
         const int tail = (extra + per_row - 1) / per_row;
@@ -1022,9 +1065,6 @@ int Engine::launch_unfused(const StepParams &p, int kind)
     } else {
         OTF_CUDA(launch_pdl(k_unfused_p_rev, dim3(U.ncb, U.nseg, 2 * n_shots_), dim3(kUThreads), st_, U,
                             n_shots_));
-        const int np = n_ring_ + U.n_rcv_cells;
-        if (np > 0)
-            OTF_CUDA(launch_pdl(k_unfused_points<true>, dim3((np + 127) / 128, n_shots_), dim3(128), st_, U));
         OTF_CUDA(launch_pdl(k_unfused_a_rev, grid, dim3(kUThreads), st_, U));
     }
     OTF_CUDA(cudaGetLastError());

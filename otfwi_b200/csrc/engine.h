@@ -200,7 +200,8 @@ class Engine {
     StreamTabs stb_{};
     // unfused kernels: per-CTA injection lists, receiver and ring offsets
     struct {
-        const int *src_ptr, *src_off, *src_id, *rcv_ptr, *rcv_off, *rcv_id, *rec_off, *ring_off;
+        const int *src_ptr, *src_off, *src_id, *src_cta, *rcv_ptr, *rcv_off, *rcv_id, *rcv_cta;
+        const int *rec_off, *ring_off, *ring_cta, *ring_cta_off, *ring_cta_k;
         int n_src_cells, n_rcv_cells, ncb, nseg;
     } utb_{};
     int n_strips_ = 0, seg_h_ = 64;

@@ -7,14 +7,14 @@
 // half-step is its own launch over the whole batch, every cell is computed
 // once, and nothing waits on anything but its own loads:
 //
-//   forward step:  P kernel  P(t), Q(t) from P, Q, Ax, Az (t-1)
-//                  points    the shot's sources injected
+//   forward step:  P kernel  P(t), Q(t) from P, Q, Ax, Az (t-1); then each
+//                            CTA injects the shot's sources in its cells
 //                  A kernel  Ax, Az (t) from P(t); extra CTAs record the
 //                            receivers and the boundary ring
 //   reverse step:  P kernel  both field sets: reconstruction (undamped,
-//                            reverted) and adjoint (damped)
-//                  points    P_rec(t) = ring(T-1-t) on the ring cells, the
-//                            adjoint sources injected at the receivers
+//                            reverted; then P_rec(t) = ring(T-1-t) on the
+//                            CTA's ring cells) and adjoint (damped; then the
+//                            adjoint sources at the CTA's receivers)
 //                  A kernel  both A updates, the 9-point Laplacian of
 //                            P_rec(t) and grad += P_adj(t) * lap
 //
@@ -49,11 +49,15 @@ struct UnfusedParams {
     int ncb, nseg;  // column blocks, row segments per shot
     // injection cells (CSR): padded offset of each distinct cell holding a
     // source / an injectable receiver, and its source / receiver indices in
-    // increasing order
-    const int *src_ptr, *src_off, *src_id;
+    // increasing order; cells grouped by the P-kernel CTA that owns them
+    // (src_cta / rcv_cta [ncb * nseg + 1] index the cell arrays)
+    const int *src_ptr, *src_off, *src_id, *src_cta;
     int n_src_cells;
-    const int *rcv_ptr, *rcv_off, *rcv_id;
+    const int *rcv_ptr, *rcv_off, *rcv_id, *rcv_cta;
     int n_rcv_cells;
+    // ring cells grouped by owning CTA: ring_cta [ncb * nseg + 1] indexes
+    // ring_cta_off (padded offset) and ring_cta_k (ring index)
+    const int *ring_cta, *ring_cta_off, *ring_cta_k;
     // padded offsets (within a shot) of the receivers and of the ring cells
     // (ring id = the caller's ring index)
     const int *rec_off, *ring_off;
@@ -84,7 +88,7 @@ __device__ __forceinline__ void ust4(float *p, const float *v)
 
 // One 4-column segment of a P half-step. REVERT: time-reversed
 // reconstruction (undamped, no Q); otherwise damped with the strip
-// component Q. Point injection follows in k_unfused_points.
+// component Q. The CTA's point work follows in the calling kernel.
 template <bool REVERT>
 __device__ __forceinline__ void p_segment(const UnfusedParams &U, const Fields &f, const float *__restrict__ q,
                                           int shot, int x, int z0)
@@ -169,34 +173,85 @@ __device__ __forceinline__ void p_segment(const UnfusedParams &U, const Fields &
     }
 }
 
+// Injection at one cell after its P update: the sources fired by the shot
+// (or the adjoint sources at a receiver), P += I (both split components get
+// I/2) and Q += I/2 on strip cells, in source order, exactly as the fused
+// kernels inject.
+__device__ __forceinline__ void inject_cell(const StepParams &p, const Fields &f, int shot, int off, const int *ids,
+                                            int e0, int e1, bool sources)
+{
+    const int64_t o = p.shot_stride * shot + off;
+    const int z = off / p.pitch - PAD, x = off - (z + PAD) * p.pitch - PAD;
+    const bool strip = __ldg(p.dampx + x + PAD) != 1.f || __ldg(p.dampz + z + PAD) != 1.f;
+    float pn = f.px_out[o], qn = strip ? f.pz_out[o] : 0.f;
+    for (int e = e0; e < e1; e++) {
+        const int row = sources ? p.fire_row[shot * p.n_src + ids[e]] : shot * p.n_sen + ids[e];
+        if (row < 0)
+            continue;
+        const float I = p.inj_tab[(int64_t)row * p.T + p.t];
+        pn = __fadd_rn(pn, I);
+        if (strip)
+            qn = __fadd_rn(qn, __fmul_rn(I, 0.5f));
+    }
+    f.px_out[o] = pn;
+    if (strip)
+        f.pz_out[o] = qn;
+}
+
+// The point work of a P-kernel CTA, after its lanes wrote P(t) (and Q(t))
+// of its cells: lanes take distinct cells, so nothing races; __syncwarp
+// orders the lanes' writes before these reads.
+__device__ __forceinline__ void cta_inject(const StepParams &p, const Fields &f, int shot, const int *cta_idx,
+                                           const int *off, const int *ptr, const int *ids, int cta, bool sources)
+{
+    for (int c = cta_idx[cta] + (int)threadIdx.x; c < cta_idx[cta + 1]; c += kUThreads)
+        inject_cell(p, f, shot, off[c], ids, ptr[c], ptr[c + 1], sources);
+}
+
 // Resident CTAs each kernel is compiled for (a register cap), from
 // measurements: 24 (80 registers) for the P kernels, 28 (72) for the forward
 // A kernel; the reverse A kernel needs its 128 registers.
 constexpr int kUPMinBlocks = 24;
 constexpr int kUAMinBlocks = 28;
 
-// Forward P half-step: grid (ncb, nseg, n_shots).
+// Forward P half-step and the sources: grid (ncb, nseg, n_shots).
 __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
-    if (x >= U.p.X)
-        return;
-    p_segment<false>(U, U.p.f0, U.p.q0, blockIdx.z, x, blockIdx.y * kURows);
+    const int cta = blockIdx.x + U.ncb * blockIdx.y;
+    if (x < U.p.X)
+        p_segment<false>(U, U.p.f0, U.p.q0, blockIdx.z, x, blockIdx.y * kURows);
+    __syncwarp();
+    cta_inject(U.p, U.p.f0, blockIdx.z, U.src_cta, U.src_off, U.src_ptr, U.src_id, cta, true);
 }
 
 // Reverse P half-steps of both sets: grid (ncb, nseg, 2 * n_shots); z <
-// n_shots: reconstruction (set 0, q0), else adjoint (set 1, q1).
+// n_shots: reconstruction (set 0, q0) then the ring overwrite, else adjoint
+// (set 1, q1) then the adjoint sources.
 __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_rev(const __grid_constant__ UnfusedParams U, int n_shots)
 {
     pdl_enter();
+    const StepParams &p = U.p;
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
-    if (x >= U.p.X)
-        return;
-    if ((int)blockIdx.z < n_shots)
-        p_segment<true>(U, U.p.f0, U.p.q0, blockIdx.z, x, blockIdx.y * kURows);
-    else
-        p_segment<false>(U, U.p.f1, U.p.q1, blockIdx.z - n_shots, x, blockIdx.y * kURows);
+    const int cta = blockIdx.x + U.ncb * blockIdx.y;
+    const bool rec_set = (int)blockIdx.z < n_shots;
+    const int shot = rec_set ? (int)blockIdx.z : (int)blockIdx.z - n_shots;
+    if (x < p.X) {
+        if (rec_set)
+            p_segment<true>(U, p.f0, p.q0, shot, x, blockIdx.y * kURows);
+        else
+            p_segment<false>(U, p.f1, p.q1, shot, x, blockIdx.y * kURows);
+    }
+    __syncwarp();
+    if (rec_set) {
+        // setRec: P_rec(t) = ring(T-1-t) on the ring cells of this CTA
+        const float *ring = p.ring + ((int64_t)shot * p.T + (p.T - 1 - p.t)) * p.n_ring;
+        for (int c = U.ring_cta[cta] + (int)threadIdx.x; c < U.ring_cta[cta + 1]; c += kUThreads)
+            p.f0.px_out[p.shot_stride * shot + U.ring_cta_off[c]] = ring[U.ring_cta_k[c]];
+    } else {
+        cta_inject(p, p.f1, shot, U.rcv_cta, U.rcv_off, U.rcv_ptr, U.rcv_id, cta, false);
+    }
 }
 
 // A update of one cell from the staggered derivatives of P(t): reverted,
@@ -411,55 +466,6 @@ __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_consta
                 wa[j][k] = wa[j][k + 1];
         }
     }
-}
-
-// Point work between the P and A kernels, one thread per (cell, shot):
-// forward (RING = false): the sources fired by the shot, P += I (both split
-// components get I/2) and Q += I/2 on strip cells, in source order, after
-// the cell's P update, exactly as the fused kernels inject; reverse (RING):
-// P_rec(t) = ring(T-1-t) on the ring cells of set 0 and the adjoint sources
-// at the receivers into set 1. grid (ceil(n / 128), n_shots).
-__device__ __forceinline__ void inject_cell(const StepParams &p, const Fields &f, int shot, int off, const int *ids,
-                                            int e0, int e1, bool sources)
-{
-    const int64_t o = p.shot_stride * shot + off;
-    const int z = off / p.pitch - PAD, x = off - (z + PAD) * p.pitch - PAD;
-    const bool strip = __ldg(p.dampx + x + PAD) != 1.f || __ldg(p.dampz + z + PAD) != 1.f;
-    float pn = f.px_out[o], qn = strip ? f.pz_out[o] : 0.f;
-    for (int e = e0; e < e1; e++) {
-        const int row = sources ? p.fire_row[shot * p.n_src + ids[e]] : shot * p.n_sen + ids[e];
-        if (row < 0)
-            continue;
-        const float I = p.inj_tab[(int64_t)row * p.T + p.t];
-        pn = __fadd_rn(pn, I);
-        if (strip)
-            qn = __fadd_rn(qn, __fmul_rn(I, 0.5f));
-    }
-    f.px_out[o] = pn;
-    if (strip)
-        f.pz_out[o] = qn;
-}
-
-template <bool RING>
-__global__ void __launch_bounds__(128) k_unfused_points(const __grid_constant__ UnfusedParams U)
-{
-    pdl_enter();
-    const StepParams &p = U.p;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int shot = blockIdx.y;
-    if (!RING) {
-        if (i < U.n_src_cells)
-            inject_cell(p, p.f0, shot, U.src_off[i], U.src_id, U.src_ptr[i], U.src_ptr[i + 1], true);
-        return;
-    }
-    if (i < p.n_ring) {
-        p.f0.px_out[p.shot_stride * shot + U.ring_off[i]] =
-            p.ring[((int64_t)shot * p.T + (p.T - 1 - p.t)) * p.n_ring + i];
-        return;
-    }
-    const int k = i - p.n_ring;
-    if (k < U.n_rcv_cells)
-        inject_cell(p, p.f1, shot, U.rcv_off[k], U.rcv_id, U.rcv_ptr[k], U.rcv_ptr[k + 1], false);
 }
 
 }  // namespace otf
