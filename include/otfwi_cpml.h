@@ -51,6 +51,12 @@ void set_source(int ns, int *ps_x, int *ps_z);
  * of every receiver from t = 0 into the buffer returned by init_memory_sim. */
 void cuda_simulate2(int en_out, int idx_source);
 
+/* Every source as its own shot (one pixel per element), all shots advanced
+ * by one launch per step (no counterpart in the reference, which runs one
+ * cuda_simulate2 per source): traces [ns][nm][T] (host), each identical to
+ * that of cuda_simulate2(0, s). Returns 0, or -1 with otf_last_error set. */
+int otf_cpml_simulate_all(float *traces);
+
 /* Exact discrete adjoint of the forward map (no counterpart in the
  * reference, which has no CPML gradient): grad_kappa [Z*X] = dL/dkappa for
  * dL/dtraces = g [nm*T] (host arrays), kappa = rho c^2 the Laplacian's

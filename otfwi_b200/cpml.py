@@ -66,6 +66,9 @@ def _declare(L):
     if hasattr(L, "otf_cpml_gradient"):
         L.otf_cpml_gradient.restype = c_int
         L.otf_cpml_gradient.argtypes = [fp, fp, c_int, c_int]
+    if hasattr(L, "otf_cpml_simulate_all"):
+        L.otf_cpml_simulate_all.restype = c_int
+        L.otf_cpml_simulate_all.argtypes = [fp]
     L._cpml_declared = True
     return L
 
@@ -137,6 +140,19 @@ class CPMLSimulator:
         self._check()
         n = self.n_rec * self.T
         return np.ctypeslib.as_array(self._rec, shape=(n,)).copy().reshape(self.n_rec, self.T)
+
+    def simulate_all(self):
+        """Traces [n_src, n_rec, T] of every source fired alone (the
+        reference's per-source loop), all shots in one launch per step (this
+        package's library only)."""
+        if not hasattr(self.L, "otf_cpml_simulate_all"):
+            raise _lib.OtfwiError("this CPML library has no batched forward")
+        out = np.zeros((self.n_src, self.n_rec, self.T), np.float32)
+        rc = self.L.otf_cpml_simulate_all(out.ctypes.data_as(POINTER(c_float)))
+        self._check()
+        if rc != 0:
+            raise _lib.OtfwiError("otf_cpml_simulate_all failed")
+        return out
 
     def gradient(self, g, idx_source=-1, checkpoint_every=None):
         """dL/dkappa [Z, X] for dL/dtraces = g [n_rec, T] (exact discrete

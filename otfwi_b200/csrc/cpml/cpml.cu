@@ -72,6 +72,10 @@ struct StepArgs {
     const float *cquad, *src;
     float qtpi;
     float *rec;
+    // batched shots (blockIdx.z = shot s, which fires source s alone): field
+    // pointers are shot 0's, shot_stride floats apart; rec is [shot][nm][T]
+    size_t shot_stride;
+    int batch;
 };
 
 __device__ __forceinline__ bool inb(int X, int Z, int x, int z) { return x >= 4 && z >= 4 && x < X - 4 && z < Z - 4; }
@@ -111,10 +115,21 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
     __shared__ float sVx[VH][VW], sVz[VH][VW];
     const int X = a.X, Z = a.Z;
     const int x0 = blockIdx.x * TX, z0 = blockIdx.y * TZ;
+    const size_t so = (size_t)blockIdx.z * a.shot_stride;
+    const float *__restrict__ P1 = a.P1 + so;
+    const float *__restrict__ P2 = a.P2 + so;
+    float *__restrict__ Pn = a.Pn + so;
+    const float *__restrict__ mx_in = a.mx_in + so;
+    const float *__restrict__ mz_in = a.mz_in + so;
+    float *__restrict__ mx_out = a.mx_out + so;
+    float *__restrict__ mz_out = a.mz_out + so;
+    float *__restrict__ mxxp = a.mxx + so;
+    float *__restrict__ mzzp = a.mzz + so;
+    float *rec = a.rec ? a.rec + (size_t)blockIdx.z * a.nm * a.T : nullptr;
     for (int k = threadIdx.x; k < SW * SH; k += NTH) {
         const int zz = k / SW, xx = k - zz * SW;
         const int x = x0 - 8 + xx, z = z0 - 8 + zz;
-        sP[zz][xx] = inb(X, Z, x, z) ? a.P1[(size_t)z * X + x] : 0.f;
+        sP[zz][xx] = inb(X, Z, x, z) ? P1[(size_t)z * X + x] : 0.f;
     }
     __syncthreads();
     // first derivatives, memory variables and density division on the tile + 4-cell halo
@@ -126,16 +141,16 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
             const size_t i = (size_t)z * X + x;
             // offset 0: taps x-3 .. x+4 (tile column of x is ex + 4)
             const float v0x = div_sp(stag<FAITHFUL>(&sP[ez + 4][ex + 1], 1), a.c.dx, a.c.inv_dx);
-            const float mx = __fmaf_rn(a.c.bxh[x], a.mx_in[i], __fmul_rn(a.c.axh[x], v0x));
+            const float mx = __fmaf_rn(a.c.bxh[x], mx_in[i], __fmul_rn(a.c.axh[x], v0x));
             const float kx = (a.c.k_one & 2) ? v0x : __fdiv_rn(v0x, a.c.Kxh[x]);
             vx = __fdiv_rn(__fadd_rn(kx, mx), a.c.rho_hx[i]);
             const float v0z = div_sp(stag<FAITHFUL>(&sP[ez + 1][ex + 4], SW), a.c.dz, a.c.inv_dz);
-            const float mz = __fmaf_rn(a.c.bzh[z], a.mz_in[i], __fmul_rn(a.c.azh[z], v0z));
+            const float mz = __fmaf_rn(a.c.bzh[z], mz_in[i], __fmul_rn(a.c.azh[z], v0z));
             const float kz = (a.c.k_one & 8) ? v0z : __fdiv_rn(v0z, a.c.Kzh[z]);
             vz = __fdiv_rn(__fadd_rn(kz, mz), a.c.rho_hz[i]);
             if (ex >= 4 && ex < TX + 4 && ez >= 4 && ez < TZ + 4) {
-                a.mx_out[i] = mx;
-                a.mz_out[i] = mz;
+                mx_out[i] = mx;
+                mz_out[i] = mz;
             }
         }
         sVx[ez][ex] = vx;
@@ -151,19 +166,19 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
         const size_t i = (size_t)z * X + x;
         // offset 1: taps x-4 .. x+3 (region column of x is ox + 4)
         const float vxx0 = div_sp(stag<FAITHFUL>(&sVx[oz + 4][ox], 1), a.c.dx, a.c.inv_dx);
-        const float mxx = __fmaf_rn(a.c.bx[x], a.mxx[i], __fmul_rn(a.c.ax[x], vxx0));
-        a.mxx[i] = mxx;
+        const float mxx = __fmaf_rn(a.c.bx[x], mxxp[i], __fmul_rn(a.c.ax[x], vxx0));
+        mxxp[i] = mxx;
         const float vxx1 = __fadd_rn((a.c.k_one & 1) ? vxx0 : __fdiv_rn(vxx0, a.c.Kx[x]), mxx);
         const float vzz0 = div_sp(stag<FAITHFUL>(&sVz[oz][ox + 4], VW), a.c.dz, a.c.inv_dz);
-        const float mzz = __fmaf_rn(a.c.bz[z], a.mzz[i], __fmul_rn(a.c.az[z], vzz0));
-        a.mzz[i] = mzz;
+        const float mzz = __fmaf_rn(a.c.bz[z], mzzp[i], __fmul_rn(a.c.az[z], vzz0));
+        mzzp[i] = mzz;
         const float vzz1 = __fadd_rn((a.c.k_one & 4) ? vzz0 : __fdiv_rn(vzz0, a.c.Kz[z]), mzz);
         const float lap = __fadd_rn(vxx1, vzz1);
-        a.Pn[i] = __fmaf_rn(__fmul_rn(lap, a.c.dt2), a.c.kappa[i], __fmaf_rn(2.f, a.P1[i], -a.P2[i]));
-        if (a.lap)
+        Pn[i] = __fmaf_rn(__fmul_rn(lap, a.c.dt2), a.c.kappa[i], __fmaf_rn(2.f, P1[i], -P2[i]));
+        if (a.lap)  // single-shot launches only
             a.lap[i] = lap;
     }
-    if (a.ns == 0 && !a.rec)
+    if (a.ns == 0 && !rec)
         return;
     // sources in this tile (somaFonte, regression_CPML.cu:210-231), then the
     // receivers in it (:238-246), by the first warp: lanes test 32 points at
@@ -174,7 +189,7 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
         return;
     const int lane = threadIdx.x;
     auto mine = [&](int px, int pz) { return px >= x0 && px < x0 + TX && pz >= z0 && pz < z0 + TZ; };
-    const int idx = a.ns > 0 ? *a.idx_dev : -1;
+    const int idx = a.batch ? (int)blockIdx.z : (a.ns > 0 ? *a.idx_dev : -1);
     for (int base = 0; base < a.ns; base += 32) {
         const int n = base + lane;
         const bool hit = n < a.ns && !(a.ppe == 1 && idx != -1 && idx != n) && mine(a.sx[n], a.sz[n]);
@@ -185,14 +200,14 @@ __global__ void __launch_bounds__(NTH) k_cpml_step(const StepArgs a)
                 m &= m - 1;
                 const size_t i = (size_t)a.sz[k] * X + a.sx[k];
                 const float sv = __fmul_rn(__fmul_rn(a.qtpi, a.cquad[i]), a.src[(size_t)k * a.T + a.t]);
-                a.Pn[i] = __fmaf_rn(sv, a.c.dt2, a.Pn[i]);
+                Pn[i] = __fmaf_rn(sv, a.c.dt2, Pn[i]);
             }
         __syncwarp();
     }
-    if (a.rec)
+    if (rec)
         for (int n = lane; n < a.nm; n += 32)
             if (mine(a.pmx[n], a.pmz[n]))
-                a.rec[(size_t)n * a.T + a.t] = a.Pn[(size_t)a.pmz[n] * X + a.pmx[n]];
+                rec[(size_t)n * a.T + a.t] = Pn[(size_t)a.pmz[n] * X + a.pmx[n]];
 }
 
 // gravaBufferSensores2ordem (regression_CPML.cu:238-246)
@@ -320,9 +335,20 @@ struct State {
     int k_one = 0;                     // K profiles that are exactly 1 (bits Kx, Kxh, Kz, Kzh)
     float *gbuf = nullptr;  // gradient work buffers, kept between calls
     size_t gbuf_floats = 0;
+    // every source as its own shot in one launch per step: per shot P [4]
+    // slots, mx, mz [2], mxx, mzz (10 fields of Z*X), traces [shot][nm][T]
+    float *bfields = nullptr, *brec = nullptr;
+    int b_shots = 0;
+    cudaGraphExec_t batch_graph = nullptr;
 
     void release()
     {
+        if (batch_graph)
+            cudaGraphExecDestroy(batch_graph);
+        if (bfields)
+            cudaFree(bfields);
+        if (brec)
+            cudaFree(brec);
         if (gbuf)
             cudaFree(gbuf);
         if (sim_graph)
@@ -497,6 +523,8 @@ static void fill_args(StepArgs &a)
     a.src = g.src;
     a.qtpi = g.qtpi;
     a.rec = nullptr;
+    a.shot_stride = 0;
+    a.batch = 0;
 }
 
 // P(0), P(1) from the initial field, every other slot and memory variable zero
@@ -596,6 +624,92 @@ static int simulate(int idx)
     OTF_CUDA(cudaGraphLaunch(g.sim_graph, st));
     if (g.nm > 0)
         OTF_CUDA(cudaMemcpyAsync(g.rec_h, g.rec_d, (size_t)g.nm * T * sizeof(float), cudaMemcpyDeviceToHost, st));
+    OTF_CUDA(cudaStreamSynchronize(st));
+    return 0;
+}
+
+// Every source as its own shot (ppe = 1), all shots in one launch per step
+// (grid z = shot): the traces of cuda_simulate2(0, s) for every s, bit for
+// bit, into rec_h [ns][nm][T]. The time loop is one graph, as in simulate.
+static int simulate_all(float *rec_h)
+{
+    OTF_CHECK(g.P != nullptr, 2, "cpml simulate_all called before init_memory_sim");
+    OTF_CHECK(g.ppe == 1, 1, "cpml simulate_all: one pixel per element only (each source its own shot)");
+    OTF_CHECK(g.ns > 0, 1, "cpml simulate_all: no sources");
+    const int X = g.X, T = g.T, S = g.ns;
+    const size_t XZ = (size_t)X * g.Z, stride = 10 * XZ;
+    cudaStream_t st = g.st;
+    if (g.b_shots != S) {
+        if (g.batch_graph)
+            cudaGraphExecDestroy(g.batch_graph);
+        g.batch_graph = nullptr;
+        if (g.bfields)
+            cudaFree(g.bfields);
+        if (g.brec)
+            cudaFree(g.brec);
+        g.bfields = g.brec = nullptr;
+        g.b_shots = 0;
+        OTF_CUDA(cudaMalloc(&g.bfields, stride * S * sizeof(float)));
+        OTF_CUDA(cudaMalloc(&g.brec, std::max<size_t>(1, (size_t)S * g.nm * T) * sizeof(float)));
+        g.b_shots = S;
+    }
+    if (!g.batch_graph) {
+        cudaGraph_t graph = nullptr;
+        OTF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int rc = 0;
+        // shot layout: P slots 0-3 | mx 0-1 | mz 0-1 | mxx | mzz
+        float *P = g.bfields, *mx = P + 4 * XZ, *mz = mx + 2 * XZ, *mxx = mz + 2 * XZ, *mzz = mxx + XZ;
+        for (int sh = 0; sh < S && rc == 0; sh++) {
+            float *b = g.bfields + (size_t)sh * stride;
+            if (cudaMemsetAsync(b, 0, stride * sizeof(float), st) != cudaSuccess ||
+                cudaMemcpyAsync(b, g.init, 2 * XZ * sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+                rc = -1;
+        }
+        StepArgs a;
+        fill_args(a);
+        a.shot_stride = stride;
+        a.batch = 1;
+        a.mxx = mxx;
+        a.mzz = mzz;
+        const dim3 grid((X + TX - 1) / TX, (g.Z + TZ - 1) / TZ, S);
+        for (int t = 0; t < T && rc == 0; t++) {
+            if (t <= 1) {
+                for (int sh = 0; sh < S && g.nm > 0; sh++)
+                    k_cpml_record<<<(g.nm + 127) / 128, 128, 0, st>>>(
+                        P + (size_t)sh * stride + (size_t)(t % 4) * XZ, X, T, t, g.nm, g.pmx, g.pmz,
+                        g.brec + (size_t)sh * g.nm * T);
+                continue;
+            }
+            a.t = t;
+            a.P1 = P + (size_t)((t + 3) % 4) * XZ;
+            a.P2 = P + (size_t)((t + 2) % 4) * XZ;
+            a.Pn = P + (size_t)(t % 4) * XZ;
+            a.mx_in = mx + (size_t)((t + 1) % 2) * XZ;
+            a.mz_in = mz + (size_t)((t + 1) % 2) * XZ;
+            a.mx_out = mx + (size_t)(t % 2) * XZ;
+            a.mz_out = mz + (size_t)(t % 2) * XZ;
+            a.rec = g.nm > 0 ? g.brec : nullptr;
+            if (g.precision == 1)
+                k_cpml_step<false><<<grid, NTH, 0, st>>>(a);
+            else
+                k_cpml_step<true><<<grid, NTH, 0, st>>>(a);
+        }
+        const cudaError_t el = cudaGetLastError();
+        const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+        if (rc || el != cudaSuccess) {
+            if (graph)
+                cudaGraphDestroy(graph);
+            OTF_CUDA(el);
+            return -1;
+        }
+        OTF_CUDA(ec);
+        const cudaError_t ei = cudaGraphInstantiate(&g.batch_graph, graph, 0);
+        cudaGraphDestroy(graph);
+        OTF_CUDA(ei);
+    }
+    OTF_CUDA(cudaGraphLaunch(g.batch_graph, st));
+    if (g.nm > 0)
+        OTF_CUDA(cudaMemcpyAsync(rec_h, g.brec, (size_t)S * g.nm * T * sizeof(float), cudaMemcpyDeviceToHost, st));
     OTF_CUDA(cudaStreamSynchronize(st));
     return 0;
 }
@@ -775,6 +889,10 @@ void set_source(int ns, int *ps_x, int *ps_z)
         return;
     }
     g.ns = ns;
+    if (g.batch_graph) {  // captured for the previous source set
+        cudaGraphExecDestroy(g.batch_graph);
+        g.batch_graph = nullptr;
+    }
     if (ns > 0 && (cudaMemcpy(g.sx, ps_x, ns * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
                    cudaMemcpy(g.sz, ps_z, ns * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess))
         otf::set_error_msg(2, "cpml set_source: copy failed");
@@ -790,6 +908,12 @@ int otf_last_status(void) { return otf::last_status(); }
 const char *otf_last_error(void) { return otf::last_error(); }
 void otf_clear_error(void) { otf::clear_error(); }
 void otf_cpml_release(void) { g.release(); }
+
+int otf_cpml_simulate_all(float *traces)
+{
+    otf::clear_error();
+    return otf::cpml::simulate_all(traces);
+}
 
 int otf_cpml_gradient(const float *g_traces, float *grad_kappa, int checkpoint_every, int idx_source)
 {

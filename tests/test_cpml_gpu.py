@@ -85,6 +85,31 @@ def test_cpml_repeated_calls_replay_one_graph():
     assert np.array_equal(seq[4], co.simulate(two, X, Z, T, idx_source=-1, ppe=ppe))
 
 
+def test_cpml_all_sources_batch_matches_per_source_calls():
+    """otf_cpml_simulate_all (every source its own shot, one launch per step)
+    against cuda_simulate2 per source: identical traces, twice in a row (the
+    captured graph replayed) and after set_source drops a source."""
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r); sys.path.insert(0, %r);"
+        "import make_cpml_golden as m; sim, idx, ppe = m.case_sim('cpml_shot1', None);"
+        "b1 = sim.simulate_all(); b2 = sim.simulate_all();"
+        "one = np.stack([sim.simulate(s) for s in range(sim.n_src)]);"
+        "from ctypes import POINTER, c_int;"
+        "x = np.ascontiguousarray(sim.inputs['ps_x'][:2]); z = np.ascontiguousarray(sim.inputs['ps_z'][:2]);"
+        "sim.L.set_source(2, x.ctypes.data_as(POINTER(c_int)), z.ctypes.data_as(POINTER(c_int))); sim._check();"
+        "sim.n_src = 2; b3 = sim.simulate_all(); two = np.stack([sim.simulate(s) for s in range(2)]);"
+        "np.savez(sys.argv[1], b1=b1, b2=b2, one=one, b3=b3, two=two)" % (ROOT, GOLDEN))
+    out = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"cpml_all_{os.getpid()}.npz")
+    subprocess.run([sys.executable, "-c", code, out], check=True)
+    d = dict(np.load(out))
+    os.remove(out)
+    assert d["one"].shape[0] == 3
+    assert np.array_equal(d["b1"], d["one"]) and np.array_equal(d["b2"], d["one"])
+    assert np.array_equal(d["b3"], d["two"])
+    g = np.load(os.path.join(GOLDEN, "cpml_shot1.npz"))
+    assert np.array_equal(d["one"][1], g["traces"])
+
+
 def test_cpml_general_spacing_and_stretching_bit_exact():
     """A spacing that is not a power of two and K profiles that are not 1
     (the step divides by both) against the oracle's reference arithmetic,
