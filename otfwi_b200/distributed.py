@@ -1,5 +1,7 @@
 """Multi-GPU FWI gradient: shots (or whole acquisitions) sharded over ranks,
-one reduction per gradient.
+one reduction per gradient; and the data-parallel step of the
+preconditioner's training (each rank its own micro-batch, one all-reduce of
+the flat parameter gradient per step).
 
 The reference runs every shot serially on one GPU (cuda_interface_pml.py:
 225-236: grad_acc += grad per shot, then / n_source). Shots are
@@ -41,3 +43,33 @@ def distributed_gradient(shot_gradient, n_shots, rank, world, shape, group=None,
         m += float(ms)
     allreduce_sum_([g, m], group=group)
     return (g / n_shots).cpu().numpy(), float(m.item())
+
+
+def world_of(group=None):
+    """(world size, rank) of an initialised process group, else (1, 0)."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return 1, 0
+    return dist.get_world_size(group), dist.get_rank(group)
+
+
+def dp_average_(grads, group=None):
+    """Data-parallel gradient: replace a flat parameter gradient by its mean
+    over ranks (one all-reduce; a no-op in a single process). With each
+    rank's loss normalised over its own micro-batch, the mean is the gradient
+    of the mean loss over the global batch."""
+    import torch.distributed as dist
+    world, _ = world_of(group)
+    if world > 1:
+        dist.all_reduce(grads, op=dist.ReduceOp.SUM, group=group)
+        grads.div_(world)
+    return grads
+
+
+def broadcast_params_(params, group=None):
+    """Rank 0's parameters on every rank (before data-parallel training)."""
+    import torch.distributed as dist
+    world, _ = world_of(group)
+    if world > 1:
+        dist.broadcast(params, src=0, group=group)
+    return params

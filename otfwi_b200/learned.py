@@ -131,21 +131,34 @@ def generate(n_runs, seed0=1000, X=256, Z=256, T=1500, n_elem=32, pitch=6, n_src
     return torch.stack(xs), torch.stack(ys), weight, stats
 
 
-def train(net, X, Y, weight, steps=4000, batch=16, lr=1e-3, seed=0, log=None):
+def train(net, X, Y, weight, steps=4000, batch=16, lr=1e-3, seed=0, log=None, group=None):
     """Adam on the weighted MSE with cosine learning-rate decay and random
-    horizontal flips; returns the loss history (host floats, every step)."""
+    horizontal flips; returns the loss history (host floats, every step).
+
+    Data parallel when a process group is initialised (one process per GPU):
+    rank 0's parameters are broadcast first, every rank draws its own
+    micro-batch of ``batch`` pairs (global batch = batch x world), and the
+    flat parameter gradient is averaged over ranks by one all-reduce before
+    each Adam step, so every rank keeps identical parameters. The loss
+    history is the mean over ranks."""
     import torch
-    g = torch.Generator(device="cuda")
-    g.manual_seed(seed)
+    from .distributed import broadcast_params_, dp_average_, world_of
+    world, rank = world_of(group)
+    dev = net.params.device
+    if world > 1:
+        broadcast_params_(net.params, group)
+        net.pack()
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 7919 * rank)
     M = X.shape[0]
     w = weight[None].expand(batch, -1, -1).contiguous()
     inv = 1.0 / float(w.sum().item())
     losses = []
     for s in range(steps):
-        idx = torch.randint(0, M, (batch,), device="cuda", generator=g)
+        idx = torch.randint(0, M, (batch,), device=dev, generator=g)
         xb = X[idx].float()
         yb = Y[idx].float()
-        flip = torch.rand(batch, device="cuda", generator=g) < 0.5
+        flip = torch.rand(batch, device=dev, generator=g) < 0.5
         xb = torch.where(flip[:, None, None, None], xb.flip(2), xb).contiguous()
         yb = torch.where(flip[:, None, None], yb.flip(2), yb).contiguous()
         wb = torch.where(flip[:, None, None], w.flip(2), w).contiguous()
@@ -153,6 +166,9 @@ def train(net, X, Y, weight, steps=4000, batch=16, lr=1e-3, seed=0, log=None):
         net.forward(xb)
         loss = net.loss_grad(yb, wb, inv_norm=inv).clone()
         net.backward(net._buffers(*yb.shape)["dout"])
+        if world > 1:
+            dp_average_(net.grads, group)
+            dp_average_(loss, group)
         net.adam(lr_s)
         losses.append(loss)
         if log and (s % 500 == 0 or s == steps - 1):
