@@ -297,6 +297,9 @@ void Engine::free_all()
         cudaFree(mscratch_);
     mscratch_ = nullptr;
     mscratch_bytes_ = 0;
+    for (void *p : retired_)
+        cudaFree(p);
+    retired_.clear();
     for (auto &a : fld_)
         for (auto &b : a)
             for (auto &c : b) {
@@ -1368,14 +1371,23 @@ int Engine::prepare_gradient(int kind)
     if (kind == kMisfitQuadEnvelope && envelope_prepare(n_shots_ * n_rec_, cfg_.T))
         return -1;
     const int64_t need = misfit_scratch_per_trace(kind, cfg_.T) * n_shots_ * n_rec_;
-    if (need > mscratch_bytes_) {
-        drop_graphs();
-        if (mscratch_)
-            OTF_CUDA(cudaFree(mscratch_));
-        mscratch_ = nullptr;
-        OTF_CUDA(cudaMalloc(&mscratch_, (size_t)need));
-        mscratch_bytes_ = need;
-    }
+    return grow_scratch(need);
+}
+
+// A larger misfit scratch: this engine's graphs are dropped (re-captured on
+// next use) and the old buffer retired, not freed, since a multi-instance
+// graph composed earlier may still reference it.
+int Engine::grow_scratch(int64_t need)
+{
+    if (need <= mscratch_bytes_)
+        return 0;
+    drop_graphs();
+    if (mscratch_)
+        retired_.push_back(mscratch_);
+    mscratch_ = nullptr;
+    mscratch_bytes_ = 0;
+    OTF_CUDA(cudaMalloc(&mscratch_, (size_t)need));
+    mscratch_bytes_ = need;
     return 0;
 }
 
@@ -1560,15 +1572,9 @@ int Engine::misfit(int kind, double *total_dev)
 {
     OTF_CHECK(ready_ && obs_, 2, "receivers not configured");
     const int n = n_shots_ * n_rec_;
-    const int64_t need = misfit_scratch_per_trace(kind, cfg_.T) * n;
-    if (need > mscratch_bytes_) {
-        if (mscratch_)
-            OTF_CUDA(cudaFree(mscratch_));
-        mscratch_ = nullptr;
-        mscratch_bytes_ = 0;
-        OTF_CUDA(cudaMalloc(&mscratch_, (size_t)need));
-        mscratch_bytes_ = need;
-    }
+    // inside a capture the gradient / objective preparation has sized it
+    if (grow_scratch(misfit_scratch_per_trace(kind, cfg_.T) * n))
+        return -1;
     if (launch_misfit(kind, rec_, obs_, adj_, mis_, n, cfg_.T, mscratch_, mscratch_bytes_, st_))
         return -1;
     if (total_dev) {

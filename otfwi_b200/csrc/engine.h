@@ -161,6 +161,11 @@ class Engine {
     double *mis_ = nullptr;                      // [max_shots*n_rec]
     void *mscratch_ = nullptr;                   // misfit CDF scratch
     int64_t mscratch_bytes_ = 0;
+    // scratch buffers outgrown while graphs (this engine's, or multi-instance
+    // graphs composed from them) may still hold their addresses: freed with
+    // the engine, never while such a graph could still run
+    std::vector<void *> retired_;
+    int grow_scratch(int64_t need);
     int *inj_src_ = nullptr;   // CSR: ptr[max_shots+1] | x | z | row
     int *inj_adj_ = nullptr;
     int *tabs_ = nullptr;      // per-tile receiver / ring tables
