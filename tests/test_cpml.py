@@ -1,14 +1,17 @@
 """CPU tests of the CPML path: the library exports every symbol its header
 declares, the profiles are the convolutional-PML recursion coefficients,
-and the oracle's reference-arithmetic mode agrees with its FP64 mode."""
+the oracle's reference-arithmetic mode is bit-identical to the reference's
+own CPML library on the committed golden cases, and it agrees with its FP64
+mode."""
 import ctypes
+import glob
 import os
 
 import numpy as np
 import pytest
 
 import cpml_oracle as co
-from conftest import ROOT
+from conftest import GOLDEN, ROOT
 
 
 def test_cpml_library_exports_header_symbols():
@@ -55,6 +58,22 @@ def _inputs(X=72, Z=64, T=250):
         for k, v in zip(("d", "K", "alpha", "a", "b"), prof):
             inp[f"{k}_{name}"] = f32(v)
     return inp, X, Z, T
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "cpml_*.npz"))), ids=os.path.basename)
+def test_cpml_oracle_pinned_to_reference(path):
+    """The oracle's reference-arithmetic mode gives every trace sample of the
+    reference's own CPML library (tests/golden/make_cpml_golden.py ran it on
+    a GPU): one shot, all sources together, odd grid sizes, two points per
+    element and an initial field; the FP64 mode stays within 1e-5."""
+    d = np.load(path)
+    X, Z, T, idx, ppe = (int(d[k]) for k in ("X", "Z", "T", "idx", "ppe"))
+    inp = {k: d[k] for k in d.files}
+    o32 = co.simulate(inp, X, Z, T, idx_source=idx, ppe=ppe)
+    assert np.array_equal(o32, d["traces"])
+    o64 = co.simulate(inp, X, Z, T, idx_source=idx, ppe=ppe, mode="f64")
+    err = float(np.abs(o64 - d["traces"]).max() / np.abs(o64).max())
+    assert err <= 1e-5, err
 
 
 def test_cpml_oracle_modes_agree_and_absorb():
