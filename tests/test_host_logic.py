@@ -1,6 +1,7 @@
 """CPU tests of host-side logic around the kernels: the uneven batch's
 instance generator and wave packing, the autotuner's candidate set and cache
-key, and the bench's reading of the committed ncu summaries."""
+key, the bench's reading of the committed ncu summaries, and the FWI loop's
+line search, history and gradient mask."""
 import importlib.util
 import os
 
@@ -57,3 +58,65 @@ def test_bench_reads_the_committed_traffic_summaries(kernel):
     if kernel == 4:
         share = b.profile_value(4, "a_rev_share_of_step")
         assert 0.3 < share < 0.9
+
+
+class _Quadratic:
+    """A stand-in for fwi.Problem along one direction: J(c) = (c - c_min)^2 + J_min
+    on a scalar model, clipped to [vmin, vmax]; counts evaluations."""
+
+    def __init__(self, c_min, J_min=0.0, vmin=-1e9, vmax=1e9):
+        self.c_min, self.J_min, self.vmin, self.vmax = c_min, J_min, vmin, vmax
+        self.calls = 0
+
+    def objective(self, b, c):
+        self.calls += 1
+        return float((c - self.c_min) ** 2 + self.J_min)
+
+    def clip(self, c):
+        return min(max(c, self.vmin), self.vmax)
+
+
+@pytest.mark.parametrize("alpha0", [0.25, 1.0, 16.0, 100.0])
+def test_line_search_brackets_and_lands_on_a_quadratic_minimum(alpha0):
+    """Expanding from a short first step or shrinking from a long one, the
+    bracket's parabolic step lands on the minimum of a quadratic (the
+    three-point vertex is exact for a parabola); the evaluation count it
+    reports is the number of objective calls."""
+    from otfwi_b200.fwi import line_search
+    prob = _Quadratic(3.0)
+    J0 = prob.objective(0, 0.0)
+    prob.calls = 0
+    a, J, evals = line_search(prob, 0, 0.0, 1.0, J0, alpha0, max_evals=12)
+    assert evals == prob.calls
+    assert abs(a - 3.0) < 1e-9 and J < 1e-12
+
+
+def test_line_search_reports_no_step_uphill():
+    """Along an ascent direction no trial decreases the misfit: step 0, the
+    starting misfit, and no more than max_evals trials."""
+    from otfwi_b200.fwi import line_search
+    prob = _Quadratic(0.0, J_min=1.0)
+    a, J, evals = line_search(prob, 0, 0.0, 1.0, 1.0, 0.5, max_evals=6)
+    assert (a, J) == (0.0, 1.0) and evals == 6 == prob.calls
+
+
+def test_line_search_respects_the_bounds():
+    """Trial models are clipped to [vmin, vmax]: a minimum beyond the upper
+    bound gives a step that reaches the bound and never a misfit below the
+    bound's."""
+    from otfwi_b200.fwi import line_search
+    prob = _Quadratic(10.0, vmax=4.0)
+    J0 = prob.objective(0, 0.0)
+    a, J, _ = line_search(prob, 0, 0.0, 1.0, J0, 1.0, max_evals=8)
+    assert prob.clip(a) == 4.0 and J == prob.objective(0, 4.0)
+
+
+def test_history_time_to_and_default_gmask():
+    from otfwi_b200 import scenarios
+    from otfwi_b200.fwi import History, default_gmask
+    h = History(t=[0.0, 1.5, 3.0], rms=[100.0, 80.0, 60.0])
+    assert h.time_to(80.0) == 1.5 and h.time_to(59.0) is None and h.time_to(1e9) == 0.0
+    sc = scenarios.small(X=96, Z=80, T=50, n_src=1, n_rec=4, seed=1)
+    m = default_gmask(sc)
+    assert m.shape == (80, 96) and m.sum() == (80 - 2 * 20) * (96 - 2 * 24)
+    assert m[20, 24] == 1 and m[19, 24] == 0 and m[20, 23] == 0 and m[59, 71] == 1 and m[60, 71] == 0
