@@ -41,6 +41,36 @@ def test_calls_before_init_report_errors_without_gpu(lib):
         _lib.check(lib)
 
 
+def test_product_entry_points_fail_loudly_without_a_gpu(lib):
+    """There is no CPU fallback: without a CUDA device every public entry
+    point (the reference wrapper's mirror, the batched shots, the
+    reference-signature misfits, the CPML simulator) raises OtfwiError."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from otfwi_b200 import _lib, adjoint_functions, scenarios
+    from otfwi_b200.batch import ShotBatch
+    from otfwi_b200.cpml import CPMLSimulator
+    from otfwi_b200.cuda_interface_pml import Cuda_interface_PML
+    sc = scenarios.small(X=96, Z=80, T=50, n_src=1, n_rec=4, seed=1)
+    calls = [
+        lambda: Cuda_interface_PML(sc.X, sc.Z, sc.T, sc.PML, sc.c_true, sc.n_src, sc.src_mask, sc.n_rec,
+                                   sc.rec_mask, sc.source, multishot=True).simulate(),
+        lambda: ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source).forward(),
+        lambda: CPMLSimulator(sc.X, sc.Z, sc.T, sc.PML, sc.c_true, sc.src_mask, sc.rec_mask, sc.source,
+                              f0=0.04).simulate(-1),
+    ]
+    tr = np.zeros((2, 16), np.float32)
+    for name in ("L2", "wasserstein", "wasserstein_softplus", "wasserstein_quad", "quad_envelope",
+                 "wasserstein_pm"):
+        calls.append(lambda f=getattr(adjoint_functions, name): f(tr, tr))
+    for call in calls:
+        with pytest.raises(_lib.OtfwiError):
+            call()
+    lib.otf_release()
+    lib.otf_clear_error()
+
+
 def _load_reference_wrapper(tmp_path, libpath):
     """Import the reference's unchanged cuda_interface_pml.py with CWD set so
     its relative 'simulator/bin/cuda_regression_PML_single.so' is this library."""
