@@ -342,6 +342,10 @@ int Engine::init(const EngineConfig &cfg, const float *d_x, const float *d_z)
     OTF_CHECK(cfg.precision == kFaithful || cfg.precision == kFast, 1, "unknown precision");
     OTF_CHECK(cfg.tile >= 0 && cfg.tile < kNumTileShapes, 1, "unknown tile shape");
     OTF_CHECK(cfg.dx != 0.f, 1, "dx must be non-zero");
+    // point tables (sources, receivers, ring cells) hold 32-bit cell offsets
+    // into one padded field slot
+    OTF_CHECK(Layout::make(cfg.X, cfg.Z).slot <= (int64_t)INT32_MAX, 1,
+              "grid too large: one padded field must stay below 2^31 cells");
     cfg_ = cfg;
     L_ = Layout::make(cfg.X, cfg.Z);
     const int X = cfg.X, Z = cfg.Z;

@@ -31,7 +31,10 @@ def save(path, recording, model, true_model, xzm, xzs, vmin, vmax, fun, mseL2, m
 
 
 def load(path):
-    """The result list of a reference or of this package as a dict keyed by FIELDS."""
+    """The result list of a reference or of this package as a dict keyed by FIELDS.
+
+    The format is a pickle, as the reference writes it, and unpickling runs
+    whatever the file tells it to: load only result files you trust."""
     with open(path, "rb") as f:
         r = pickle.load(f)
     if not isinstance(r, list) or len(r) != len(FIELDS):

@@ -41,6 +41,25 @@ def test_calls_before_init_report_errors_without_gpu(lib):
         _lib.check(lib)
 
 
+def test_oversized_grid_is_refused_before_any_input_is_read(lib):
+    """A 46400 x 46400 grid pads to more than 2^31 cells per field, past the
+    32-bit cell offsets of the point tables: init_memory_sim records an error
+    before it reads an input array (one-element arrays stand in for them)."""
+    import ctypes
+    from ctypes import POINTER, c_float, c_int
+    lib.otf_release()
+    lib.otf_clear_error()
+    one_f = (c_float * 3)(1.0, 1.0, 1.0)
+    one_i = (c_int * 1)(20)
+    rec = POINTER(c_float)()
+    lib.init_memory_sim(46400, 46400, 100, one_f, one_f, one_f, one_f, 1, one_i, one_i, 1, one_i, one_i,
+                        one_f, None, ctypes.byref(rec))
+    assert lib.otf_last_status() != 0
+    assert b"grid too large" in lib.otf_last_error()
+    lib.otf_release()
+    lib.otf_clear_error()
+
+
 def test_product_entry_points_fail_loudly_without_a_gpu(lib):
     """There is no CPU fallback: without a CUDA device every public entry
     point (the reference wrapper's mirror, the batched shots, the
