@@ -48,13 +48,20 @@ def _load():
 
 
 def _store(d):
+    """Write the cache through a per-process temporary file and an atomic
+    rename, so ranks tuning at the same time never leave a torn file."""
     p = cache_path()
+    tmp = f"{p}.{os.getpid()}.tmp"
     try:
         os.makedirs(os.path.dirname(p), exist_ok=True)
-        with open(p, "w") as f:
+        with open(tmp, "w") as f:
             json.dump(d, f, indent=1, sort_keys=True)
+        os.replace(tmp, p)
     except OSError:
-        pass
+        try:
+            os.remove(tmp)
+        except OSError:
+            pass
 
 
 def time_config(sc, kernel, tile, precision, T_proxy, misfit, reps=2):

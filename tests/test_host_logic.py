@@ -43,6 +43,26 @@ def test_autotune_candidates_and_cache_key():
     assert all(t in autotune.TILES for _, t in fast + faithful)
 
 
+def test_autotune_cache_round_trip_and_unwritable_location(tmp_path, monkeypatch):
+    """The cache survives a store/load round trip with no temporary file left
+    behind; an unreadable or unwritable location degrades to an empty cache
+    instead of an error; a torn file reads as empty."""
+    from otfwi_b200 import autotune
+    p = tmp_path / "tune" / "tune.json"
+    monkeypatch.setenv("OTFWI_TUNE_CACHE", str(p))
+    entry = {"k": {"kernel": 4, "tile": 4, "table": {"4/4": 118.1}}}
+    autotune._store(entry)
+    assert autotune._load() == entry
+    assert [f.name for f in p.parent.iterdir()] == ["tune.json"]
+    p.write_text('{"k": {"kernel"')
+    assert autotune._load() == {}
+    blocker = tmp_path / "file"
+    blocker.write_text("")
+    monkeypatch.setenv("OTFWI_TUNE_CACHE", str(blocker / "sub" / "tune.json"))
+    autotune._store(entry)  # the directory cannot be made: silently skipped
+    assert autotune._load() == {}
+
+
 def _bench():
     spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
     mod = importlib.util.module_from_spec(spec)
