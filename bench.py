@@ -204,6 +204,10 @@ def run_ours(args):
     if args.tile < 0:
         from otfwi_b200.autotune import autotune, TILES
         k, t, table = autotune(sc, precision=args.precision, misfit=args.misfit)
+        if world > 1:
+            # every rank tunes (the GPUs stay in step); all run rank 0's choice
+            from otfwi_b200.distributed import agree_ints
+            k, t = agree_ints([k, t], device=torch.device("cuda", local))
         if args.kernel < 0:
             args.kernel = k
         args.tile = t

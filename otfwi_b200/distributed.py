@@ -73,3 +73,18 @@ def broadcast_params_(params, group=None):
     if world > 1:
         dist.broadcast(params, src=0, group=group)
     return params
+
+
+def agree_ints(values, group=None, device="cpu"):
+    """Rank 0's list of small integers on every rank (one broadcast; the
+    values themselves in a single process). Used so that every rank runs the
+    kernel variant and tile shape that rank 0's autotuner chose, whatever the
+    timing noise of each rank's own tuning."""
+    import torch
+    import torch.distributed as dist
+    world, _ = world_of(group)
+    if world == 1:
+        return [int(v) for v in values]
+    t = torch.tensor([int(v) for v in values], dtype=torch.int64, device=device)
+    dist.broadcast(t, src=0, group=group)
+    return [int(v) for v in t.cpu().tolist()]

@@ -152,6 +152,31 @@ def test_data_parallel_training_two_gloo_ranks(tmp_path):
     np.testing.assert_allclose(d[0]["params"], [0.5, -1.0, 2.0], atol=0.5)
 
 
+def _agree_worker(rank, world, port, out):
+    import torch.distributed as dist
+    from otfwi_b200.distributed import agree_ints
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # each rank's own autotuner result differs (timing noise); rank 0's wins
+        got = agree_ints([4 - 2 * rank, 4 + rank])
+        np.save(os.path.join(out, f"agree{rank}.npy"), np.array(got))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_ranks_agree_on_rank0_tuning(tmp_path):
+    """bench.py's multi-rank run: every rank ends with rank 0's (kernel,
+    tile), so all GPUs of a scaling run execute the same kernels."""
+    import torch.multiprocessing as mp
+    from otfwi_b200.distributed import agree_ints
+    assert agree_ints([4, 3]) == [4, 3]  # no process group: unchanged
+    port = _free_port()
+    mp.start_processes(_agree_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    for r in range(2):
+        assert np.load(tmp_path / f"agree{r}.npy").tolist() == [4, 4]
+
+
 def test_training_single_process_unchanged():
     """Without a process group the loop is the single-GPU one: no collective."""
     from otfwi_b200 import learned
