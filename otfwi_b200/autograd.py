@@ -12,7 +12,6 @@ forward recomputed once during the backward sweep.
 import ctypes
 import math
 
-import numpy as np
 
 from . import _lib
 from .batch import ShotBatch, _declare

@@ -11,7 +11,7 @@ Arrays may be numpy (host) or torch CUDA tensors (device); results come back
 in the same kind as requested.
 """
 import ctypes
-from ctypes import POINTER, c_double, c_float, c_int, c_longlong, c_void_p
+from ctypes import POINTER, c_float, c_int, c_longlong, c_void_p
 
 import numpy as np
 

@@ -5,7 +5,6 @@ it unchanged; host-side set-up logic matches the reference. No compute calls
 import importlib.util
 import os
 import shutil
-import sys
 
 import numpy as np
 import pytest

@@ -8,13 +8,11 @@ Tolerances: adjoint gradient vs FP64 oracle adjoint, relative L2 <= 1e-4
 FD error ~1e-8), relative 1e-4 (measured <= 1.5e-6).
 """
 import os
-import sys
 
 import numpy as np
 import pytest
 
 import pml_oracle as po
-from conftest import ROOT
 
 pytestmark = pytest.mark.gpu
 
