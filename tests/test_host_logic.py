@@ -1,7 +1,8 @@
 """CPU tests of host-side logic around the kernels: the uneven batch's
 instance generator and wave packing, the autotuner's candidate set and cache
 key, the bench's reading of the committed ncu summaries, and the FWI loop's
-line search, history and gradient mask."""
+line search, history and gradient mask, and that the integration guide names
+only what the package has."""
 import importlib.util
 import os
 
@@ -140,3 +141,22 @@ def test_history_time_to_and_default_gmask():
     m = default_gmask(sc)
     assert m.shape == (80, 96) and m.sum() == (80 - 2 * 20) * (96 - 2 * 24)
     assert m[20, 24] == 1 and m[19, 24] == 0 and m[20, 23] == 0 and m[59, 71] == 1 and m[60, 71] == 0
+
+
+def test_integration_guide_names_exist():
+    """Every package name the integration guide's examples use exists, so the
+    guide cannot drift from the API."""
+    import re
+    import importlib
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    used = set(re.findall(r"from (otfwi_b200(?:\.\w+)?) import ([\w, ]+)", text))
+    assert used
+    for mod, names in used:
+        m = importlib.import_module(mod)
+        for n in (x.split(" as ")[0].strip() for x in names.split(",")):
+            assert hasattr(m, n) or importlib.util.find_spec(f"{mod}.{n}") is not None, (mod, n)
+    for mod, attr in re.findall(r"\b(fwi|learned|results|autotune)\.(\w+)\(", text):
+        assert hasattr(importlib.import_module(f"otfwi_b200.{mod}"), attr), (mod, attr)
+    for cls, meth in (("ShotBatch", "frames"), ("ShotBatch", "objective"), ("ShotBatch", "illumination"),
+                      ("MultiBatch", "gradient")):
+        assert hasattr(getattr(importlib.import_module("otfwi_b200.batch"), cls), meth)
