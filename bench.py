@@ -356,7 +356,9 @@ def run_ours(args):
                 "gpu_launches": args.steps * ((4 if args.kernel == 4 else 2) * (sc.T - 1) + 4),
                 "clocks": clk.summary(),
                 "misfit_value": float(mis.item())}
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:
+            # the host-core baseline is one figure for the job, taken at N = 1
+            # only (the other ranks would wait for it at the closing barrier)
             line["cpu_baseline"] = cpu_baseline(args, sc)
         print(json.dumps(line), flush=True)
     b.close()
