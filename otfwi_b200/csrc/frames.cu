@@ -206,6 +206,8 @@ int Engine::frames(int every, int shot, FrameSink sink, void *ctx)
         rc = emit_forward(false, on_step, &r);
         if (rc == 0)
             rc = sync();
+        else
+            cudaStreamSynchronize(stream());  // a failed sink leaves steps queued that write r.dev
     }
     cudaFree(r.dev);
     cudaFree(r.stats);
