@@ -115,11 +115,11 @@ def build_oracle():
     r = subprocess.run(["make", "-C", odir, "all"], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
-    ref = os.environ.get("OTFWI_REF", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "simulator", "src")):
-        r = subprocess.run(["make", "-C", odir, "ref", f"REF={ref}"], capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"reference build failed:\n{r.stdout}\n{r.stderr}")
+    # the recipe knows where the reference tree lies (OTFWI_REF overrides it)
+    # and builds nothing where it is absent
+    r = subprocess.run(["make", "-C", odir, "ref-if-present"], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference build failed:\n{r.stdout}\n{r.stderr}")
 
 
 if __name__ == "__main__":

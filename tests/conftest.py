@@ -9,7 +9,21 @@ for p in (ROOT, os.path.join(ROOT, "oracle")):
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE = os.environ.get("OTFWI_REF", "/root/reference")
+
+
+def _reference_tree():
+    """The reference tree the oracle recipe reads (OTFWI_REF overrides it);
+    tests that need it skip where it is absent."""
+    import subprocess
+    env = os.environ.get("OTFWI_REF")
+    if env:
+        return env
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "print-ref"],
+                       capture_output=True, text=True)
+    return r.stdout.strip() if r.returncode == 0 else ""
+
+
+REFERENCE = _reference_tree()
 
 
 def pytest_configure(config):

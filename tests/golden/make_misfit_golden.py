@@ -16,6 +16,7 @@ last as written (its negative-part CDFs are built from the positive parts).
     python tests/golden/make_misfit_golden.py --ref /path/to/Otfwi
 """
 import argparse
+import subprocess
 import os
 import sys
 import types
@@ -63,9 +64,13 @@ def make_case(rng, n_tr, T, f0, neg_excursion=False):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference tree (default: the oracle recipe's REF)")
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
     args = ap.parse_args()
+    if args.ref is None:
+        root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+        args.ref = subprocess.run(["make", "-s", "-C", os.path.join(root, "oracle"), "print-ref"],
+                                  capture_output=True, text=True, check=True).stdout.strip()
     _install_shims()
     sys.path.insert(0, args.ref)
     import adjoint_functions as adj  # the reference module, unchanged
