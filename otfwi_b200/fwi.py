@@ -16,7 +16,12 @@ scipy's L-BFGS-B with bounds [vmin, vmax], with the model misfit
   is a forward-only evaluation (``ShotBatch.objective``);
 - ``descent`` with a ``proposer`` (the learned preconditioner) first tries
   the proposed update and keeps it only if the misfit decreases, otherwise
-  it takes the plain line-search step from the same gradient.
+  it takes the plain line-search step from the same gradient;
+- with a process group of several ranks (one per GPU), each band's shots
+  are split over the ranks (``distributed.ShardedShots``): every rank models
+  and back-propagates its own block of shots, and one all-reduce per
+  gradient (and per line-search evaluation) gives every rank the same
+  gradient and misfit, so the model updates stay identical on all ranks.
 Models are nondimensional velocities c*dt/dx, as the reference's ABI takes.
 """
 import time
@@ -60,9 +65,12 @@ class Problem:
     on the GPU from the true model (synthetic, noise-free)."""
 
     def __init__(self, sc, bands, misfit="wasserstein", shots=None, precision=1, gmask=None, vmin=None,
-                 vmax=None, illum_every=8):
+                 vmax=None, illum_every=8, group=None):
         import torch
+        from .distributed import world_of
         self.torch = torch
+        self.group = group
+        self.world, self.rank = world_of(group)
         self.sc, self.bands, self.misfit = sc, list(bands), misfit
         self.shots, self.precision, self.illum_every = shots, precision, illum_every
         c_lo = float(min(sc.c_true.min(), sc.c_start.min()))
@@ -83,15 +91,30 @@ class Problem:
         return np.repeat(w[None, :], sc.n_src, axis=0)
 
     def batch(self, b):
-        """ShotBatch of band b with its observed data set."""
+        """ShotBatch of band b with its observed data set (with several
+        ranks: this rank's block of the shots behind a ShardedShots)."""
         if b not in self._batches:
             sc = self.sc
-            sb = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, self.wavelets(self.bands[b].f0_hz),
-                           shots=self.shots, precision=self.precision)
+            wav = self.wavelets(self.bands[b].f0_hz)
+            if self.world > 1:
+                from .batch import fmc_shots
+                from .distributed import ShardedShots
+                ptr, srcs = self.shots if self.shots is not None else fmc_shots(sc.n_src)
+                sb = ShardedShots(lambda shots: ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, wav,
+                                                          shots=shots, precision=self.precision),
+                                  ptr, srcs, (sc.Z, sc.X), group=self.group,
+                                  device=self.torch.device("cuda", self.torch.cuda.current_device()))
+                n_local = sb.n_local
+                n_rec = int(sc.n_rec)
+            else:
+                sb = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, wav, shots=self.shots,
+                               precision=self.precision)
+                n_local, n_rec = sb.n_shots, sb.n_rec
             sb.set_model(self.c_true)
-            obs = self.torch.empty((sb.n_shots, sb.n_rec, sc.T), dtype=self.torch.float32, device="cuda")
-            sb.forward(out=obs)
-            sb.set_observed(obs)
+            obs = self.torch.empty((n_local, n_rec, sc.T), dtype=self.torch.float32, device="cuda")
+            if n_local > 0:
+                sb.forward(out=obs)
+                sb.set_observed(obs)
             sb._obs_dev = obs
             self._batches[b] = sb
         return self._batches[b]

@@ -184,3 +184,100 @@ def test_training_single_process_unchanged():
     net = _LinearNet(3, seed=1)
     losses = learned.train(net, X, Y, w, steps=10, batch=2, lr=0.05, seed=5)
     assert len(losses) == 10 and losses[-1] < losses[0]
+
+
+class _OracleBatch:
+    """CPU stand-in with ShotBatch's interface for a shot table (ptr, srcs),
+    computed by the CPU oracle (the checker): forward traces, observed data,
+    gradient = shot mean over its shots, misfit = sum; L2 misfit."""
+
+    def __init__(self, shots):
+        sc, *_ = _problem()
+        self.Z, self.X = sc.Z, sc.X
+        ptr, srcs = shots
+        self.srcs = [int(srcs[ptr[i]]) for i in range(len(ptr) - 1)]  # one firing source per shot
+        self.cq = None
+        self.obs = None
+
+    def set_model(self, c=None, cquad=None):
+        self.cq = np.asarray(c, np.float64) ** 2 if cquad is None else np.asarray(cquad)
+
+    def set_observed(self, obs):
+        self.obs = np.asarray(obs)
+
+    def forward(self, out=None):
+        sc, dxp, dzp, sx, sz, mx, mz, rx, rz = _problem()
+        return np.stack([po.simulate(self.cq, np.ones(3), dxp, dzp, sx, sz, sc.source, mx, mz, s, "f32")
+                         for s in self.srcs])
+
+    def gradient(self, misfit="l2"):
+        sc, dxp, dzp, sx, sz, mx, mz, rx, rz = _problem()
+        g = np.zeros((self.Z, self.X))
+        m = 0.0
+        for i, s in enumerate(self.srcs):
+            gs, _, ms = po.grad(self.cq, np.ones(3), dxp, dzp, sx, sz, sc.source, mx, mz, rx, rz,
+                                lambda sim, o=self.obs[i]: mo.L2(sim, o), s, "f32")
+            g += gs
+            m += ms
+        return g / len(self.srcs), m
+
+    def objective(self, misfit="l2"):
+        sim = self.forward()
+        return float(sum(mo.L2(sim[i].astype(np.float64), self.obs[i])[0] for i in range(len(self.srcs))))
+
+
+def _sharded_worker(rank, world, port, out):
+    import torch.distributed as dist
+    from otfwi_b200.distributed import ShardedShots
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sc, *_ = _problem()
+        sh = ShardedShots(_OracleBatch, np.arange(4), np.arange(3), (sc.Z, sc.X))
+        sh.set_model(sc.c_true)
+        obs = sh.forward()
+        sh.set_observed(obs)
+        sh.set_model(sc.c_start)
+        g, m = sh.gradient("l2")
+        j = sh.objective("l2")
+        np.savez(os.path.join(out, f"sh{rank}.npz"), g=g.numpy(), m=m.numpy(), j=j, lo=sh.lo, hi=sh.hi)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shard_block_partitions():
+    from otfwi_b200.distributed import shard_block
+    for n in (0, 1, 5, 64):
+        for w in (1, 2, 3, 8):
+            blocks = [shard_block(n, w, r) for r in range(w)]
+            assert blocks[0][0] == 0 and blocks[-1][1] == n
+            assert all(blocks[r][1] == blocks[r + 1][0] for r in range(w - 1))
+            sizes = [hi - lo for lo, hi in blocks]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        shard_block(4, 2, 2)
+
+
+def test_sharded_acquisition_two_gloo_ranks(tmp_path):
+    """One 3-shot acquisition split over two gloo ranks by ShardedShots (the
+    FWI loop's multi-GPU path): each rank models only its block (shots 0-1 /
+    2), and the all-reduced gradient and misfit on every rank equal the
+    single-process shot mean and total (FP32 rounding of the rescaled local
+    means)."""
+    import torch.multiprocessing as mp
+    port = _free_port()
+    mp.start_processes(_sharded_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    ref_g = np.zeros((64, 72))
+    ref_m = 0.0
+    for s in range(3):
+        g, m = _shot_grad(s)
+        ref_g += g
+        ref_m += m
+    ref_g /= 3
+    d = [np.load(tmp_path / f"sh{r}.npz") for r in range(2)]
+    assert (int(d[0]["lo"]), int(d[0]["hi"]), int(d[1]["lo"]), int(d[1]["hi"])) == (0, 2, 2, 3)
+    assert np.array_equal(d[0]["g"], d[1]["g"]) and float(d[0]["m"][0]) == float(d[1]["m"][0])
+    np.testing.assert_allclose(d[0]["g"], ref_g, rtol=0, atol=1e-6 * np.abs(ref_g).max())
+    assert abs(float(d[0]["m"][0]) - ref_m) <= 1e-6 * abs(ref_m)
+    assert abs(float(d[0]["j"]) - ref_m) <= 1e-6 * abs(ref_m)
