@@ -207,11 +207,16 @@ int otf_misfit(int kind, const float *sim, const float *obs, float *adj, double 
  * they cannot afford cudaMalloc/cudaFree, which may synchronise the device.
  * The scratch is a 16 MiB array built into the library (held on every GPU
  * that loads it until exit); n_traces * otf_misfit_scratch_bytes(kind, 1, T)
- * above 16 MiB is rejected with an error (returns -1). The first call on a
- * device looks the array's device address up: make it before any stream
- * capture. All calls share the array: calls that may overlap on the GPU race,
- * so order them on one stream. Inputs and outputs are caller device memory.
- * Kind 4 (quad_envelope) is refused: its FFT plans allocate. */
+ * above 16 MiB is rejected with an error (returns -1). The first call in a
+ * context (again after a cudaDeviceReset) looks the array's device address
+ * up: make it before any stream capture. Under CUDA's default lazy module
+ * loading the array is placed when the library's misfit module is first used
+ * in a context (this call's first run, or an earlier otf_misfit), which needs
+ * 16 MiB of free device memory at that moment; CUDA_MODULE_LOADING=EAGER
+ * places it when the context is created instead. All calls share the array:
+ * calls that may overlap on the GPU race, so order them on one stream.
+ * Inputs and outputs are caller device memory. Kind 4 (quad_envelope) is
+ * refused: its FFT plans allocate. */
 int otf_misfit_noalloc(int kind, const float *sim, const float *obs, float *adj, double *misfit,
                        int n_traces, int T, void *stream);
 

@@ -567,39 +567,84 @@ int launch_misfit(int kind, const float *sim, const float *obs, float *adj, doub
 // 16 MiB until the process exits.
 //
 // Host code cannot use the array's name as a device address (in host code it
-// names a host-side stand-in), so its device address is looked up once per
-// device, with that device current, by cudaGetSymbolAddress. That set-up is
-// done by the first otf_misfit_noalloc call on each device; make that first
-// call before any stream capture. All calls share the one array and it keeps
-// whatever the last call left there; the kernel writes every scratch element
-// it reads, so nothing has to be cleared between calls. Calls whose kernels
-// may run at the same time on the GPU (different streams without ordering
-// between them) race on the array: serialise them.
+// names a host-side stand-in), so its device address is looked up with
+// cudaGetSymbolAddress, with the device current, and remembered per device
+// together with the id of the context it was looked up in: a context that
+// was destroyed and made again (cudaDeviceReset, which the reference's own
+// init_memory_sim calls) reloads the module and may place the array
+// elsewhere, so a changed context id triggers a new lookup. The lookup is
+// done by the first otf_misfit_noalloc call in each context; make that call
+// before any stream capture. Under CUDA's default lazy module loading, the
+// first use of this file's kernels or of the array in a context (this entry
+// point's first call, or an earlier otf_misfit call) loads the module and
+// places the 16 MiB array then: at that moment the device needs 16 MiB free
+// (CUDA_MODULE_LOADING=EAGER places it when the context is created). All
+// calls share the one array and it keeps whatever the last call left there;
+// the kernel writes every scratch element it reads, so nothing has to be
+// cleared between calls. Calls whose kernels may run at the same time on the
+// GPU (different streams without ordering between them) race on the array:
+// serialise them.
+#include <cuda.h>
 #include <mutex>
 #include <string>
 
 namespace {
 constexpr long long kNoAllocScratchBytes = 16ll << 20;
-__device__ __align__(256) char g_noalloc_misfit_scratch[kNoAllocScratchBytes];
+static __device__ __align__(256) char g_noalloc_misfit_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
-void *g_noalloc_addr[kMaxDevices] = {};
+struct NoAllocSlot {
+    unsigned long long ctx_id;
+    void *addr;
+};
+NoAllocSlot g_noalloc_slot[kMaxDevices] = {};
 
-// device address of the scratch array on the current device (looked up once)
+// the driver's context queries, through the runtime (the library does not
+// link the driver library itself, so that it loads on hosts without one)
+int context_id(unsigned long long *id)
+{
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *p = nullptr, *q = nullptr;
+        cudaDriverEntryPointQueryResult r1, r2;
+        OTF_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r1));
+        OTF_CUDA(cudaGetDriverEntryPoint("cuCtxGetId", &q, cudaEnableDefault, &r2));
+        OTF_CHECK(p && q && r1 == cudaDriverEntryPointSuccess && r2 == cudaDriverEntryPointSuccess, 1,
+                  "otf_misfit_noalloc: driver context queries unavailable");
+        get_current = reinterpret_cast<GetCurrent>(p);
+        get_id = reinterpret_cast<GetId>(q);
+    }
+    CUcontext ctx = nullptr;
+    OTF_CHECK(get_current(&ctx) == CUDA_SUCCESS && ctx != nullptr, 1, "otf_misfit_noalloc: no current CUDA context");
+    OTF_CHECK(get_id(ctx, id) == CUDA_SUCCESS, 1, "otf_misfit_noalloc: context id lookup failed");
+    return 0;
+}
+
+// device address of the scratch array in the current context
 int noalloc_scratch(void **out)
 {
     int dev = -1;
     OTF_CUDA(cudaGetDevice(&dev));
     OTF_CHECK(dev >= 0 && dev < kMaxDevices, 1, "otf_misfit_noalloc: device index out of range");
+    // make the device's primary context current (created if need be)
+    OTF_CUDA(cudaSetDevice(dev));
+    unsigned long long id = 0;
+    if (context_id(&id))
+        return -1;
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    NoAllocSlot &s = g_noalloc_slot[dev];
+    if (!s.addr || s.ctx_id != id) {
         void *p = nullptr;
         OTF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_misfit_scratch));
         OTF_CHECK(p != nullptr, 1, "otf_misfit_noalloc: scratch address lookup returned null");
-        g_noalloc_addr[dev] = p;
+        s.addr = p;
+        s.ctx_id = id;
     }
-    *out = g_noalloc_addr[dev];
+    *out = s.addr;
     return 0;
 }
 }  // namespace

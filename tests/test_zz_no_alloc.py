@@ -4,8 +4,9 @@ or they cannot afford cudaMalloc's device synchronisation). It uses the
 16 MiB scratch array built into the library instead of caller scratch.
 
 Checked through the C ABI against otf_misfit (caller-provided scratch) on
-two calls in a row with different inputs, so a second call cannot pass on
-what the first left in the shared array; and an oversize request must be
+three calls in a row with different inputs -- the last smaller than the one
+before, with another trace length -- so no call can pass on what an earlier
+one left in the shared array; and an oversize request must be
 refused with an error before anything is launched. This file is collected
 last so that a run stopping at the first failure has run every other test.
 """
@@ -52,10 +53,15 @@ def _call(lib, fn_name, kind, sim, obs, torch):
     return rc, mis.cpu().numpy(), adj.cpu().numpy()
 
 
-@pytest.mark.parametrize("kind", [1, 2, 0])
+# L2, wasserstein, softplus wasserstein, wasserstein_quad, wasserstein_pm (its
+# scratch layout differs: 5T float-float values per trace); quad_envelope is
+# refused by the entry point
+@pytest.mark.parametrize("kind", [1, 2, 0, 3, 5])
 def test_noalloc_misfit_matches_allocating_entry_point_twice(lib, kind):
     torch = pytest.importorskip("torch")
-    for call, (seed, n, T) in enumerate([(11, 24, 1500), (12, 40, 4000)]):
+    # the third call is smaller than the second and uses another T: it runs
+    # over scratch that the larger call left behind
+    for call, (seed, n, T) in enumerate([(11, 24, 1500), (12, 40, 4000), (14, 7, 977)]):
         sim, obs = _traces(seed, n, T)
         rc0, m0, a0 = _call(lib, "otf_misfit", kind, sim, obs, torch)
         rc1, m1, a1 = _call(lib, "otf_misfit_noalloc", kind, sim, obs, torch)
