@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--T", type=int, default=4000)
     ap.add_argument("--shots", type=int, default=64)
     ap.add_argument("--misfit", default="wasserstein_softplus")
+    ap.add_argument("--mode", default="weak", choices=["weak", "strong"],
+                    help="weak: every rank inverts its own 64-shot acquisition (default); strong: the shots "
+                         "of ONE acquisition split over the ranks (distributed.ShardedShots' partition)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-shots", type=int, default=2, help="shots per reference-arm step")
     ap.add_argument("--leg", default="gradient", choices=["gradient", "cpml", "misfits"],
@@ -74,12 +77,14 @@ def workload(args, rank=0):
                          x_first=max(24, args.X // 2 - 3 * args.shots + 3) + 2 * rank)
 
 
-def config_block(args, sc, parallelism):
+def config_block(args, sc, world=1):
+    """The workload's description, identical for both arms at the same N."""
     return {"workload": f"fmc{sc.X}x{sc.Z}_T{sc.T}_{sc.n_src}shots_{sc.n_rec}rx_{args.misfit}",
             "grid": [sc.X, sc.Z], "nt": sc.T, "pml": sc.PML, "shots": sc.n_src, "receivers": sc.n_rec,
             "misfit": args.misfit, "precision": ["faithful", "fast"][args.precision],
             "l2": "working set (fields of 64 shots, about 1.2 GB) larger than the 126 MB L2; no flush needed",
-            "parallelism": parallelism}
+            "parallelism": (f"shots of one acquisition over {world} GPU(s)" if args.mode == "strong"
+                            else f"one acquisition per GPU, {world} GPU(s)")}
 
 
 class Clocks:
@@ -179,13 +184,39 @@ def cpu_baseline(args, sc):
     args0 = (sc.c_true ** 2, np.ones(3), dxp, dzp, sx[:1], sz[:1], src, mx, mz)
     obs = po.simulate(*args0, mode="f32")
     t0 = time.perf_counter()
-    po.grad(sc.c_start ** 2, np.ones(3), dxp, dzp, sx[:1], sz[:1], src, mx, mz, rx, rz,
-            lambda s: mo.wasserstein_softplus(s, obs), mode="f64")
+    g64, rec64, _ = po.grad(sc.c_start ** 2, np.ones(3), dxp, dzp, sx[:1], sz[:1], src, mx, mz, rx, rz,
+                            lambda s: mo.wasserstein_softplus(s, obs), mode="f64")
     dt = time.perf_counter() - t0
     v = 2 * sc.X * sc.Z * (Ts - 1) / dt / 1e9
-    return {"value": v, "unit": UNIT, "cores": po.num_threads(), "kind": "port",
+    base = {"value": v, "unit": UNIT, "cores": po.num_threads(), "kind": "port",
             "sample": f"FP64 oracle (oracle/pml_oracle.c, OpenMP) + numpy softplus-W2 misfit: 1 shot, "
                       f"{sc.X}x{sc.Z}, first {Ts} of {sc.T} steps, forward + adjoint gradient, {dt:.1f} s"}
+    return base, {"Ts": Ts, "obs": obs, "g64": g64, "rec64": rec64}
+
+
+def err_vs_fp64(args, sc, sample):
+    """The benched numerics (same kernel variant and tile, fast or faithful)
+    on the baseline's sample -- shot 0, the first Ts steps, the same observed
+    traces and misfit -- against the FP64 oracle's traces and gradient:
+    max over receivers of max_t|d| / max_t|ref| and relative L2."""
+    from otfwi_b200.batch import ShotBatch
+    Ts = sample["Ts"]
+    b = ShotBatch(sc.X, sc.Z, Ts, sc.PML, sc.src_mask, sc.rec_mask, np.ascontiguousarray(sc.source[:, :Ts]),
+                  prec_deriv=4, precision=args.precision, tile=max(args.tile, 0), kernel=args.kernel,
+                  shots=(np.array([0, 1]), np.array([0])))
+    b.set_observed(sample["obs"][None])
+    b.set_model(sc.c_start)
+    sim = b.forward()[0]
+    g, _ = b.gradient(args.misfit)
+    b.close()
+    ref, rg = np.asarray(sample["rec64"])[:, 1:], np.asarray(sample["g64"])
+    den = np.abs(ref).max(axis=1)
+    den[den == 0] = 1.0
+    et = float((np.abs(sim[:, 1:] - ref).max(axis=1) / den).max())
+    eg = float(np.linalg.norm(g - rg) / np.linalg.norm(rg))
+    return {"trace_max_rel": et, "grad_rel_l2": eg,
+            "sample": f"shot 0, first {Ts} steps, benched kernels vs FP64 oracle (oracle/pml_oracle.c)",
+            "full_size_check": "tests/test_benchmark_configs_gpu.py (T = 4000, shots 0 and 63)"}
 
 
 def run_ours(args):
@@ -198,8 +229,16 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     from otfwi_b200.batch import ShotBatch
-    from otfwi_b200.distributed import allreduce_sum_
-    sc = workload(args, rank)
+    from otfwi_b200.distributed import allreduce_sum_, shard_block
+    strong = args.mode == "strong"
+    sc = workload(args, 0 if strong else rank)
+    shots, n_local = None, sc.n_src
+    if strong:
+        # this rank's contiguous block of the acquisition's shots
+        lo, hi = shard_block(sc.n_src, world, rank)
+        if hi <= lo:
+            raise SystemExit(f"rank {rank}: no shots left for it ({sc.n_src} shots over {world} ranks)")
+        shots, n_local = (np.arange(hi - lo + 1), np.arange(lo, hi)), hi - lo
     tuned = None
     if args.tile < 0:
         from otfwi_b200.autotune import autotune, TILES
@@ -213,13 +252,13 @@ def run_ours(args):
         args.tile = t
         tuned = {"kernel": k, "tile": list(TILES[t]), "candidates_ms_T300": table}
     b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, prec_deriv=4,
-                  precision=args.precision, tile=args.tile, kernel=args.kernel)
+                  precision=args.precision, tile=args.tile, kernel=args.kernel, shots=shots)
     b.set_stream_rows(args.stream_rows)
     dev = torch.device("cuda", local)
     stream = torch.cuda.ExternalStream(b.stream(), device=dev)
     c_true = torch.tensor(sc.c_true, dtype=torch.float32, device=dev)
     c0 = torch.tensor(sc.c_start, dtype=torch.float32, device=dev)
-    obs = torch.empty((sc.n_src, sc.n_rec, sc.T), dtype=torch.float32, device=dev)
+    obs = torch.empty((n_local, sc.n_rec, sc.T), dtype=torch.float32, device=dev)
     b.set_model(cquad=(c_true * c_true).contiguous())
     b.forward(out=obs)
     b.set_observed(obs)
@@ -230,9 +269,13 @@ def run_ours(args):
     def step():
         b.gradient(args.misfit, grad=grad, misfit_out=mis)
         if world > 1:
-            # the FWI gradient is the sum over every rank's acquisition: one
-            # NCCL all-reduce of the X*Z gradient and the misfit per step
+            # weak: the FWI gradient is the sum over every rank's acquisition;
+            # strong: the shot mean of one acquisition (local means weighted
+            # by their shot counts). One NCCL all-reduce of the X*Z gradient
+            # and the misfit per step either way.
             with torch.cuda.stream(stream):
+                if strong:
+                    grad.mul_(n_local / sc.n_src)
                 allreduce_sum_([grad, mis])
 
     for _ in range(args.warmup):
@@ -254,8 +297,8 @@ def run_ours(args):
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    cells = 2 * sc.X * sc.Z * (sc.T - 1) * sc.n_src
-    value = cells * world / (ms / 1e3) / 1e9
+    job_cells = 2 * sc.X * sc.Z * (sc.T - 1) * (sc.n_src if strong else sc.n_src * world)
+    value = job_cells / (ms / 1e3) / 1e9
 
     # per-kernel live timing of the two step kernels (graphs of T-1 launches
     # each), for the roofline of the dominant kernel
@@ -274,7 +317,7 @@ def run_ours(args):
     b._lib.otf_batch_misfit(b._h, 2, None, 0)
     ms_rev = time_graph(lambda: b._lib.otf_batch_reverse(b._h, None, 0, None, 1.0, 0))
     peak, peak_kind = measured_peak()
-    per_launch_cells = sc.X * sc.Z * sc.n_src
+    per_launch_cells = sc.X * sc.Z * n_local
     ach_rev = BYTES_REV * per_launch_cells / (ms_rev / 1e3) / 1e9
     ach_fwd = BYTES_FWD * per_launch_cells / (ms_fwd / 1e3) / 1e9
     tr = profile_traffic(args.kernel)
@@ -292,7 +335,7 @@ def run_ours(args):
             "forward_kernel": {"achieved": round(ach_fwd, 1), "frac": round(ach_fwd / peak, 4),
                                "launch_ms": round(ms_fwd, 4),
                                "algorithmic_bytes_per_launch": BYTES_FWD * per_launch_cells},
-            "whole_step_frac": round(BYTES_STEP * sc.X * sc.Z * (sc.T - 1) * sc.n_src
+            "whole_step_frac": round(BYTES_STEP * sc.X * sc.Z * (sc.T - 1) * n_local
                                      / (ms / 1e3) / 1e9 / peak, 4)}
     share = profile_value(args.kernel, "a_rev_share_of_step") if args.kernel == 4 else None
     if share:
@@ -316,9 +359,11 @@ def run_ours(args):
     def e2e_step():
         b.set_model(cquad=h_cq.numpy())
         b.set_observed(h_obs.numpy())
-        b._ok(b._lib.otf_batch_gradient(b._h, 2, __import__("ctypes").c_void_p(h_grad.data_ptr()),
-                                        __import__("ctypes").c_void_p(h_mis.data_ptr()), 0))
-        b.sync()
+        step()  # gradient on the device (and, with several ranks, its all-reduce)
+        with torch.cuda.stream(stream):
+            h_grad.copy_(grad, non_blocking=True)
+            h_mis.copy_(mis, non_blocking=True)
+        stream.synchronize()
 
     for _ in range(max(1, args.warmup // 2)):
         e2e_step()
@@ -337,18 +382,18 @@ def run_ours(args):
         t = torch.tensor([ms_e2e], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_e2e = float(t.item())
-    e2e = {"value": cells * world / (ms_e2e / 1e3) / 1e9, "unit": UNIT,
+    e2e = {"value": job_cells / (ms_e2e / 1e3) / 1e9, "unit": UNIT,
            "h2d_bytes_per_step": int(h_cq.numel() * 4 + h_obs.numel() * 4),
            "d2h_bytes_per_step": int(h_grad.numel() * 4 + 8), "ms_per_step": round(ms_e2e, 3)}
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "higher_is_better": True, "scaling": args.mode, "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded model, Ricker source; no external dataset)",
-                "config": dict(config_block(args, sc, f"shots-per-rank, gradient all-reduce, {world} rank(s)"),
-                               kernel_variant=args.kernel, tile=args.tile, autotune=tuned,
-                               stream_rows=args.stream_rows if args.kernel == 3 else None),
+                "config": config_block(args, sc, world),
+                "tuning": {"kernel_variant": args.kernel, "tile": args.tile, "autotune": tuned,
+                           "stream_rows": args.stream_rows if args.kernel == 3 else None},
                 "roofline": roof, "e2e": e2e,
                 # per time step one fused launch forward and one reverse (the
                 # unfused variant 4: a P and an A launch in each); per
@@ -359,7 +404,8 @@ def run_ours(args):
         if not args.no_cpu_baseline and world == 1:
             # the host-core baseline is one figure for the job, taken at N = 1
             # only (the other ranks would wait for it at the closing barrier)
-            line["cpu_baseline"] = cpu_baseline(args, sc)
+            line["cpu_baseline"], sample = cpu_baseline(args, sc)
+            line["err_vs_fp64"] = err_vs_fp64(args, sc, sample)
         print(json.dumps(line), flush=True)
     b.close()
     if world > 1:
@@ -384,7 +430,7 @@ def run_reference(args):
     from otfwi_b200.cuda_interface_pml import Cuda_interface_PML
     path = os.path.join(ROOT, "oracle", "_ref", "cuda_regression_PML_single.so")
     sc = workload(args)
-    cfg = config_block(args, sc, "reference per-shot loop, 1 GPU")
+    cfg = config_block(args, sc)
     if not os.path.exists(path):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref library not built"}))
         return
@@ -397,7 +443,13 @@ def run_reference(args):
         cp._lib.cuda_simulate(0, s)
         ctypes.memmove(buf.ctypes.data, cp.recptr[0], buf.nbytes)
         obs[s] = buf
-    cp.init_regression(obs, mo.wasserstein, prec_deriv=4)
+    # the same trace misfit as this library's arm: the reference recipe
+    # (adjoint_functions.wasserstein, restated) or, for the softplus variant
+    # the reference lacks, its numpy definition -- a host callback either way,
+    # as the reference wrapper runs its misfits
+    host_misfit = {"wasserstein": mo.wasserstein, "wasserstein_softplus": mo.wasserstein_softplus,
+                   "l2": mo.L2, "wasserstein_quad": mo.wasserstein_quad}[args.misfit]
+    cp.init_regression(obs, host_misfit, prec_deriv=4)
     cp._set_c_quad(sc.c_start ** 2)
 
     def step():
@@ -414,8 +466,8 @@ def run_reference(args):
     dt = (time.perf_counter() - t0) / args.steps
     value = 2 * sc.X * sc.Z * (sc.T - 1) * ns / dt / 1e9
     sample = (f"reference CUDA library (regression_PML_single.cu built by oracle/Makefile) on the GPU, "
-              f"per-shot cuda_grad_ext with the host Wasserstein callback (reference recipe; the "
-              f"reference has no softplus variant): {ns} of {sc.n_src} shots per step")
+              f"per-shot cuda_grad_ext with the host {args.misfit} callback (numpy; the reference's "
+              f"wrapper runs its misfits on the host): {ns} of {sc.n_src} shots per step")
     print(json.dumps({"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": 1,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 2),
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

@@ -6,15 +6,17 @@ on a CUDA GPU, through its C ABI in the call sequence the reference wrapper
 uses (tests/abi_driver.py). It must run in a process of its own: the
 reference calls cudaDeviceReset() in init_memory_sim.
 
-Cases are small seeded problems (X a multiple of 32, which keeps the
-reference's unguarded somaFrames / calcGrad2 writes inside each row). Each
+Cases are small seeded problems, plus the plain single-shot benchmark
+configuration at its full size (256 x 256, T = 1500; ``c1``), all with X a
+multiple of 32, which keeps the reference's unguarded somaFrames / calcGrad2
+writes inside each row. Each
 file holds the inputs and the reference's outputs:
   traces_all / traces_s<k>  cuda_simulate(0, -1) / cuda_simulate(0, k)
   grad_s<k>                 cuda_grad_ext, L2 adjoint source against data
                             from the true model, at the start model
   sim_s<k>                  the traces the reference handed to the callback
 
-    python tests/golden/make_sim_golden.py --out /tmp/golden
+    python tests/golden/make_sim_golden.py --out /tmp/golden [--cases c1]
 """
 import argparse
 import ctypes
@@ -64,14 +66,27 @@ def cases():
     return out
 
 
+def benchmark_cases():
+    """The plain single-shot configuration at its full size: 256 x 256, 20-cell
+    PML, T = 1500, one 5 MHz Ricker source at the top-surface centre, 32
+    receivers at pitch 8 on the same row, three seeded 3000 m/s circular
+    defects in 5900 m/s, gradient at the homogeneous 5900 m/s start."""
+    sc = scenarios.plain_single_shot()
+    return {"c1": case_inputs(sc, *pml_damping(sc.X, sc.Z, sc.PML), np.ones(3))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--lib", default=os.path.join(ROOT, "oracle", "_ref", "cuda_regression_PML_single.so"))
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--cases", default="all", help="comma-separated case names (default: every case)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     lib = _declare(ctypes.CDLL(os.path.abspath(args.lib)))
-    for name, inp in cases().items():
+    todo = dict(cases(), **benchmark_cases())
+    if args.cases != "all":
+        todo = {k: todo[k] for k in args.cases.split(",")}
+    for name, inp in todo.items():
         res = run_abi(lib, **inp)
         path = os.path.join(args.out, f"sim_{name}.npz")
         np.savez_compressed(path, **inp, **res)
