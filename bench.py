@@ -157,7 +157,7 @@ def profile_traffic(kernel):
 def profile_value(kernel, key):
     """A 'key: N' line of the committed ncu summary of the reverse step of
     this kernel variant (None when absent)."""
-    name = "reverse_step_unfused_fmc.md" if kernel == 4 else "reverse_step_fmc.md"
+    name = {4: "reverse_step_unfused_fmc.md", 5: "reverse_step_paired_fmc.md"}.get(kernel, "reverse_step_fmc.md")
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
@@ -321,7 +321,10 @@ def run_ours(args):
     ach_rev = BYTES_REV * per_launch_cells / (ms_rev / 1e3) / 1e9
     ach_fwd = BYTES_FWD * per_launch_cells / (ms_fwd / 1e3) / 1e9
     tr = profile_traffic(args.kernel)
-    if args.kernel == 4:
+    if args.kernel == 5:
+        rev_name = ("k_paired_rev (reverse step in one launch: adjoint + reconstruction + imaging "
+                    "condition, all shots)")
+    elif args.kernel == 4:
         rev_name = ("reverse step (k_unfused_p_rev + k_unfused_a_rev: adjoint + reconstruction + "
                     "imaging condition, all shots; 88 B/cell moved)")
     else:
@@ -398,7 +401,8 @@ def run_ours(args):
                 # per time step one fused launch forward and one reverse (the
                 # unfused variant 4: a P and an A launch in each); per
                 # gradient the misfit, its sum, the running integral, shot mean
-                "gpu_launches": args.steps * ((4 if args.kernel == 4 else 2) * (sc.T - 1) + 4),
+                "gpu_launches": args.steps * ((4 if args.kernel == 4 else 2) * (sc.T - 1) + 4
+                                              + (2 if args.kernel == 5 else 0)),
                 "clocks": clk.summary(),
                 "misfit_value": float(mis.item())}
         if not args.no_cpu_baseline and world == 1:

@@ -91,6 +91,13 @@ int otf_set_precision(int precision);
 int otf_set_tile(int tile);
 /* Free every buffer of the drop-in state. */
 void otf_release(void);
+/* Exercises the failure reporting of the paired step kernels' device-side
+ * synchronisation without any GPU fault: one bounded wait on a counter that
+ * nothing increments (it gives up after its 0.5 s limit) and one check of a
+ * ticket count against a wrong expectation. Writes the error bits the device
+ * recorded to *bits (2 = a dependency wait timed out, 4 = tickets out of
+ * range); returns 0 when both were reported, -1 otherwise. */
+int otf_selftest_paired_faults(int *bits);
 
 /* ---- Part 3: batched shots (additive) -----------------------------------
  * Replaces the per-shot loops of Cuda_interface_PML.simulate / calc_grad
@@ -121,15 +128,23 @@ int otf_batch_set_model(otf_batch *b, const float *cquad, int on_device);       
 int otf_batch_set_observed(otf_batch *b, const float *obs, int on_device);      /* [n_shots*n_rec*T] */
 int otf_batch_set_precision(otf_batch *b, int precision);
 int otf_batch_set_tile(otf_batch *b, int tile);
-/* -1 (default): automatic, 2 with fast numerics and 1 otherwise; 0: one
- * tile per CTA per step; 1: persistent CTAs with TMA double-buffered halo
- * tiles (tile shapes 0, 1 and 4; others use 0); 2: persistent strip-split
- * kernels, fast numerics only (tile shapes 0, 1 and 4); 3: z-streaming
- * strips of 120 columns, fast numerics, separable damping, X a multiple of 4
- * (else 2). 0 and 1 give bit-identical results. */
+/* -1 (default): automatic -- 5 with fast numerics and separable damping, 2
+ * with fast numerics otherwise, 1 with faithful numerics; 0: one tile per
+ * CTA per step; 1: persistent CTAs with TMA double-buffered halo tiles (tile
+ * shapes 0, 1 and 4; others use 0); 2: persistent strip-split kernels, fast
+ * numerics only (tile shapes 0, 1 and 4); 3: z-streaming strips of 120
+ * columns, fast numerics, separable damping, X a multiple of 4 (else 2); 4:
+ * unfused half-steps, a launch each, fast numerics, separable damping; 5:
+ * paired half-steps, both in one launch per step (P and A work items handed
+ * out in order by a ticket counter), fast numerics, separable damping. 0 and
+ * 1 give bit-identical results, and so do 4 and 5. */
 int otf_batch_set_kernel(otf_batch *b, int variant);
 /* Rows per segment of the z-streaming kernels (variant 3; default 64, >= 8). */
 int otf_batch_set_stream_rows(otf_batch *b, int rows);
+/* Paired kernels (variant 5): P work items issued before the first A item
+ * (0, the default: one generation of resident CTAs; clamped to [2 column
+ * blocks, all P items]). */
+int otf_batch_set_paired_lead(otf_batch *b, int lead);
 /* Forward modelling of every shot; traces [n_shots][n_rec][T] (NULL: keep). */
 int otf_batch_forward(otf_batch *b, float *traces, int on_device);
 /* Forward with boundary-ring recording (gradient phase 1). */

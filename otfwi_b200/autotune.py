@@ -9,7 +9,8 @@ so the search runs once per configuration.
 
 Candidates: tile shapes 0 (56x56), 1 (120x24), 4 (56x24) with the persistent
 TMA kernels (variant 1) and, for the fast numerics, the strip-split kernels
-(variant 2) and the unfused streaming half-steps (variant 4, no tiles);
+(variant 2), the unfused streaming half-steps (variant 4, no tiles) and the
+paired half-steps (variant 5, both in one launch, no tiles);
 shapes 2 (120x56) and 3 (248x24) with the one-tile-per-CTA kernels
 (variant 0).
 """
@@ -25,7 +26,7 @@ TILES = {0: (56, 56), 1: (120, 24), 2: (120, 56), 3: (248, 24), 4: (56, 24)}
 def candidates(precision):
     c = [(1, 0), (1, 1), (1, 4), (0, 2), (0, 3)]
     if precision == 1:
-        c = [(4, 4), (2, 0), (2, 1), (2, 4)] + c
+        c = [(5, 4), (4, 4), (2, 0), (2, 1), (2, 4)] + c
     return c
 
 

@@ -39,6 +39,7 @@ def _declare(lib):
         "otf_batch_set_tile": [c_void_p, c_int],
         "otf_batch_set_kernel": [c_void_p, c_int],
         "otf_batch_set_stream_rows": [c_void_p, c_int],
+        "otf_batch_set_paired_lead": [c_void_p, c_int],
         "otf_batch_forward": [c_void_p, c_void_p, c_int],
         "otf_batch_forward_ring": [c_void_p, c_void_p, c_int],
         "otf_batch_gradient": [c_void_p, c_int, c_void_p, c_void_p, c_int],
@@ -187,8 +188,14 @@ class ShotBatch:
         """-1: automatic; 0: one tile per CTA per step; 1: persistent
         TMA-pipelined CTAs; 2: persistent strip-split kernels (fast numerics);
         3: z-streaming strips (fast numerics); 4: unfused streaming
-        half-steps (fast numerics)."""
+        half-steps (fast numerics); 5: paired half-steps, one launch per
+        step (fast numerics)."""
         self._ok(self._lib.otf_batch_set_kernel(self._h, variant))
+
+    def set_paired_lead(self, lead):
+        """P items issued before the first A item by the paired kernels
+        (variant 5); 0 = one generation of resident CTAs."""
+        self._ok(self._lib.otf_batch_set_paired_lead(self._h, int(lead)))
 
     def set_stream_rows(self, rows):
         """Rows per segment of the z-streaming kernels (variant 3)."""

@@ -11,6 +11,7 @@
 #include "engine.h"
 #include "misfit.h"
 #include "pml_step_unfused.cuh"
+#include "pml_step_paired.cuh"
 
 namespace otf {
 
@@ -316,6 +317,10 @@ void Engine::free_all()
     if (derr_)
         cudaFree(derr_);
     derr_ = nullptr;
+    if (pair_sync_)
+        cudaFree(pair_sync_);
+    pair_sync_ = nullptr;
+    pair_sync_bytes_ = 0;
     if (ckpt_)
         cudaFree(ckpt_);
     if (seg_)
@@ -839,6 +844,27 @@ int Engine::build_tables()
             h.push_back(e[2]);
         h.push_back(0);
     }
+    // every receiver (recording), grouped the same way: cta [NC + 1], offset,
+    // receiver index
+    const size_t o_urec = h.size();
+    {
+        std::vector<std::array<int, 3>> rc;  // (cta, offset, receiver index)
+        for (int n = 0; n < n_rec_; n++)
+            rc.push_back({cta_of(rec_x_[n], rec_z_[n]), (int)L_.at(rec_x_[n], rec_z_[n]), n});
+        std::sort(rc.begin(), rc.end());
+        std::vector<int> cta(NC + 1, 0);
+        for (auto &e : rc)
+            cta[e[0] + 1]++;
+        for (int c = 0; c < NC; c++)
+            cta[c + 1] += cta[c];
+        h.insert(h.end(), cta.begin(), cta.end());
+        for (auto &e : rc)
+            h.push_back(e[1]);
+        h.push_back(0);
+        for (auto &e : rc)
+            h.push_back(e[2]);
+        h.push_back(0);
+    }
     const size_t o_uoff = h.size();
     for (int n = 0; n < n_rec_; n++)
         h.push_back((int)L_.at(rec_x_[n], rec_z_[n]));
@@ -936,8 +962,24 @@ int Engine::build_tables()
     utb_.n_rcv_cells = n_ucells[1];
     utb_.rec_off = d + o_uoff;
     utb_.ring_off = utb_.rec_off + n_rec_;
+    utb_.rec_cta = d + o_urec;
+    utb_.rec_cta_off = utb_.rec_cta + NC + 1;
+    utb_.rec_cta_id = utb_.rec_cta_off + n_rec_ + 1;
     utb_.ncb = NCB;
     utb_.nseg = NSEG;
+    {
+        // paired kernels' counters: the ticket (first 256 bytes), then the
+        // done counts of every (shot, row segment)
+        const size_t need = 256 + sizeof(unsigned) * (size_t)std::max(cfg_.max_shots, n_shots_) * NSEG;
+        if (need > pair_sync_bytes_) {
+            if (pair_sync_)
+                cudaFree(pair_sync_);
+            pair_sync_ = nullptr;
+            pair_sync_bytes_ = 0;
+            OTF_CUDA(cudaMalloc(&pair_sync_, need));
+            pair_sync_bytes_ = need;
+        }
+    }
     tables_dirty_ = false;
     drop_graphs();
     return 0;
@@ -1005,9 +1047,13 @@ int Engine::variant_in_use() const
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
     if (variant_ == 3 && cfg_.precision == kFast && sep_ && cfg_.X % 4 == 0)
         return 3;
-    // the unfused streaming half-steps are the default of the fast numerics
-    // (separable damping), measured fastest on every grid tried
-    if ((variant_ == 4 || variant_ < 0) && cfg_.precision == kFast && sep_)
+    // the paired kernels (both half-steps of a step in one launch, P and A
+    // items ordered by tickets) are the default of the fast numerics
+    // (separable damping); the unfused ones (a launch per half-step) run the
+    // same device functions and stay selectable
+    if ((variant_ == 5 || variant_ < 0) && cfg_.precision == kFast && sep_)
+        return 5;
+    if (variant_ == 4 && cfg_.precision == kFast && sep_)
         return 4;
     return resolve_variant(k, variant_ >= 3 ? 2 : variant_, cfg_.precision);
 }
@@ -1040,7 +1086,7 @@ static cudaError_t launch_pdl(void (*kernel)(A...), dim3 grid, dim3 block, cudaS
 // sources) then A (with the receiver / ring recording CTAs); reverse P of
 // both sets (with the ring overwrite and the adjoint sources), then A of
 // both sets with the imaging condition.
-int Engine::launch_unfused(const StepParams &p, int kind)
+UnfusedParams Engine::unfused_params(const StepParams &p, int kind) const
 {
     UnfusedParams U;
     U.p = p;
@@ -1062,6 +1108,12 @@ int Engine::launch_unfused(const StepParams &p, int kind)
     U.rec_off = utb_.rec_off;
     U.ring_off = utb_.ring_off;
     U.record_ring = kind == 1;
+    return U;
+}
+
+int Engine::launch_unfused(const StepParams &p, int kind)
+{
+    const UnfusedParams U = unfused_params(p, kind);
     const dim3 grid(U.ncb, U.nseg, n_shots_);
     if (kind < 2) {
         OTF_CUDA(launch_pdl(k_unfused_p_fwd, grid, dim3(kUThreads), st_, U));
@@ -1074,6 +1126,72 @@ int Engine::launch_unfused(const StepParams &p, int kind)
                             n_shots_));
         OTF_CUDA(launch_pdl(k_unfused_a_rev, grid, dim3(kUThreads), st_, U));
     }
+    OTF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// Paired launches (pml_step_paired.cuh): one per step, P and A items of
+// every shot handed out by tickets; register caps per direction as the
+// unfused kernels (the reverse A items need their 128 registers).
+constexpr int kPairFwdMinBlocks = 24;
+constexpr int kPairRevMinBlocks = 16;
+
+int Engine::paired_lead(int kind) const
+{
+    const int ncb = utb_.ncb, np = utb_.ncb * utb_.nseg * n_shots_;
+    int lead = pair_lead_;
+    if (lead <= 0) {
+        // about one generation of resident CTAs: the awaited P items have
+        // mostly finished, their data is still in L2
+        int dev = 0, nsm = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        lead = nsm * (kind < 2 ? kPairFwdMinBlocks : kPairRevMinBlocks);
+    }
+    return std::max(std::min(lead, np), std::min(2 * ncb, np));
+}
+
+int Engine::launch_paired(const StepParams &p, int kind)
+{
+    PairedParams Q;
+    Q.U = unfused_params(p, kind);
+    Q.ticket = reinterpret_cast<unsigned long long *>(pair_sync_);
+    Q.done = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(pair_sync_) + 256);
+    Q.err = derr_;
+    Q.n_shots = n_shots_;
+    Q.lead = paired_lead(kind);
+    Q.rec_cta = utb_.rec_cta;
+    Q.rec_cta_off = utb_.rec_cta_off;
+    Q.rec_cta_id = utb_.rec_cta_id;
+    const unsigned n_items = 2u * (unsigned)(Q.U.ncb * Q.U.nseg * n_shots_);
+    if (kind < 2)
+        OTF_CUDA(launch_pdl(k_paired_fwd<kPairFwdMinBlocks>, dim3(n_items), dim3(kUThreads), st_, Q));
+    else
+        OTF_CUDA(launch_pdl(k_paired_rev<kPairRevMinBlocks>, dim3(n_items), dim3(kUThreads), st_, Q));
+    OTF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// Before a time loop of step launches: the paired kernels' tickets and done
+// counts start from zero.
+int Engine::begin_steps()
+{
+    if (variant_in_use() != 5)
+        return 0;
+    const size_t need = 256 + sizeof(unsigned) * (size_t)n_shots_ * utb_.nseg;
+    OTF_CHECK(pair_sync_ && need <= pair_sync_bytes_, 2, "paired-kernel counters not allocated");
+    OTF_CUDA(cudaMemsetAsync(pair_sync_, 0, need, st_));
+    return 0;
+}
+
+// After a loop of n_steps step launches: every paired ticket handed out once.
+int Engine::end_steps(int n_steps)
+{
+    if (variant_in_use() != 5 || n_steps <= 0)
+        return 0;
+    const unsigned long long per = 2ull * utb_.ncb * utb_.nseg * n_shots_;
+    k_paired_check<<<1, 1, 0, st_>>>(reinterpret_cast<const unsigned long long *>(pair_sync_),
+                                     per * (unsigned long long)n_steps, derr_);
     OTF_CUDA(cudaGetLastError());
     return 0;
 }
@@ -1118,6 +1236,8 @@ int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, 
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
     const int v = variant_in_use();
+    if (v == 5)
+        return launch_paired(p, with_ring ? 1 : 0);
     if (v == 4)
         return launch_unfused(p, with_ring ? 1 : 0);
     if (v == 3)
@@ -1153,6 +1273,8 @@ int Engine::launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
     const int v = variant_in_use();
+    if (v == 5)
+        return launch_paired(p, 2);
     if (v == 4)
         return launch_unfused(p, 2);
     if (v == 3)
@@ -1220,7 +1342,7 @@ int Engine::set_stream_rows(int rows)
 
 int Engine::set_variant(int variant)
 {
-    OTF_CHECK(variant >= -1 && variant <= 4, 1, "unknown kernel variant");
+    OTF_CHECK(variant >= -1 && variant <= 5, 1, "unknown kernel variant");
     if (variant != variant_) {
         variant_ = variant;
         drop_graphs();
@@ -1252,6 +1374,8 @@ int Engine::emit_forward(bool with_ring, StepHook hook, void *ctx)
     for (int f = 0; f < 4; f++)
         for (int s = 0; s < 2; s++)
             OTF_CUDA(cudaMemsetAsync(fld_[0][f][s], 0, fbytes, st_));
+    if (begin_steps())
+        return -1;
     for (int t = 1; t < cfg_.T; t++) {
         const int i = (t - 1) & 1, o = t & 1;
         p.t = t;
@@ -1262,7 +1386,7 @@ int Engine::emit_forward(bool with_ring, StepHook hook, void *ctx)
         if (hook && hook(ctx, t, o))
             return -1;
     }
-    return 0;
+    return end_steps(cfg_.T - 1);
 }
 
 // Emit the reverse time loop: running integral of the time-flipped adjoint
@@ -1289,6 +1413,8 @@ int Engine::emit_reverse()
         for (int s = 0; s < 2; s++)
             OTF_CUDA(cudaMemsetAsync(fld_[1][f][s], 0, fbytes, st_));
     OTF_CUDA(cudaMemsetAsync(grad_, 0, fbytes, st_));
+    if (begin_steps())
+        return -1;
     for (int t = 1; t < T; t++) {
         // reconstruction starts from P(T-1) (slot (T-1)%2) and A(T-2)
         // (slot (T-2)%2) (regression_PML_single.cu:787-790) and ping-pongs
@@ -1303,7 +1429,7 @@ int Engine::emit_reverse()
         if (launch_reverse_step(p, grid, pi, ai, i))
             return -1;
     }
-    return 0;
+    return end_steps(T - 1);
 }
 
 // Capture whatever `emit` puts on the stream into an instantiated graph.
@@ -1477,6 +1603,8 @@ int Engine::illumination(int every)
         for (int f = 0; f < 4; f++)
             for (int s = 0; s < 2; s++)
                 OTF_CUDA(cudaMemsetAsync(fld_[0][f][s], 0, fbytes, st_));
+        if (begin_steps())
+            return -1;
         for (int t = 1; t < cfg_.T; t++) {
             const int i = (t - 1) & 1, o = t & 1;
             p.t = t;
@@ -1490,7 +1618,7 @@ int Engine::illumination(int every)
                 OTF_CUDA(cudaGetLastError());
             }
         }
-        return 0;
+        return end_steps(cfg_.T - 1);
     };
     if (!g_illum_ && capture(&g_illum_, emit))
         return -1;
@@ -1549,7 +1677,14 @@ int Engine::sync()
         OTF_CUDA(cudaMemcpy(&h, derr_, sizeof(int), cudaMemcpyDeviceToHost));
         if (h) {
             OTF_CUDA(cudaMemset(derr_, 0, sizeof(int)));
-            OTF_CHECK(false, 5, "a bounded wait for tensor-memory copies timed out in a step kernel");
+            std::string m;
+            if (h & kErrWaitTimeout)
+                m += "a bounded wait for tensor-memory copies timed out in a step kernel; ";
+            if (h & kErrDepTimeout)
+                m += "a paired step kernel's wait for the P half-step of its neighbour rows timed out; ";
+            if (h & kErrTicketRange)
+                m += "paired step launches ran out of order or not at all (work tickets out of range); ";
+            OTF_CHECK(false, 5, m + "results of this call are invalid");
         }
     }
     return 0;
@@ -1589,3 +1724,45 @@ int Engine::misfit(int kind, double *total_dev)
 }
 
 }  // namespace otf
+
+namespace {
+__global__ void k_selftest_wait(const unsigned *cnt, int *err)
+{
+    if (threadIdx.x == 0)
+        otf::wait_geq(cnt, 1u, err);
+}
+}  // namespace
+
+extern "C" int otf_selftest_paired_faults(int *bits)
+{
+    otf::clear_error();
+    OTF_CHECK(bits != nullptr, 1, "otf_selftest_paired_faults: bits is null");
+    *bits = 0;
+    void *buf = nullptr;
+    cudaStream_t st = nullptr;
+    int rc = -1, h = 0;
+    if (cudaMalloc(&buf, 256) == cudaSuccess && cudaMemset(buf, 0, 256) == cudaSuccess &&
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) {
+        unsigned *cnt = reinterpret_cast<unsigned *>(buf);
+        int *err = reinterpret_cast<int *>(reinterpret_cast<char *>(buf) + 128);
+        auto *ticket = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(buf) + 64);
+        k_selftest_wait<<<1, 32, 0, st>>>(cnt, err);
+        otf::k_paired_check<<<1, 1, 0, st>>>(ticket, 1ull, err);
+        if (cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess &&
+            cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess) {
+            *bits = h;
+            rc = (h & otf::kErrDepTimeout) && (h & otf::kErrTicketRange) ? 0 : -1;
+            if (rc)
+                otf::set_error_msg(5, "otf_selftest_paired_faults: a fault path was not reported");
+        } else {
+            otf::set_error_msg(5, "otf_selftest_paired_faults: CUDA call failed");
+        }
+    } else {
+        otf::set_error_msg(3, "otf_selftest_paired_faults: set-up failed");
+    }
+    if (st)
+        cudaStreamDestroy(st);
+    if (buf)
+        cudaFree(buf);
+    return rc;
+}

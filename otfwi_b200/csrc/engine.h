@@ -13,6 +13,8 @@
 
 namespace otf {
 
+struct UnfusedParams;  // pml_step_unfused.cuh
+
 enum Precision : int { kFaithful = 0, kFast = 1 };
 
 // Tile shapes compiled into the library (owned cells per CTA).
@@ -107,9 +109,13 @@ class Engine {
     // -1 automatic (default); 0 one tile per CTA; 1 persistent TMA-pipelined;
     // 2 persistent strip-split (fast numerics); 3 z-streaming strips (fast
     // numerics, separable damping, X a multiple of 4); 4 unfused streaming
-    // half-steps (fast numerics, separable damping). Falls back where not
-    // compiled or not applicable.
+    // half-steps (fast numerics, separable damping); 5 paired half-steps, one
+    // launch per step (fast numerics, separable damping). Falls back where
+    // not compiled or not applicable.
     int set_variant(int variant);
+    // paired kernels: P items issued before the first A item (0 = one
+    // generation of resident CTAs)
+    void set_paired_lead(int lead) { pair_lead_ = lead; drop_graphs(); }
     // rows per segment of the z-streaming kernels (>= 8)
     int set_stream_rows(int rows);
     int variant_in_use() const;
@@ -132,6 +138,11 @@ class Engine {
     int launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain, int in1);
     int launch_stream(const StepParams &p, int kind);  // 0 forward, 1 forward + ring, 2 reverse
     int launch_unfused(const StepParams &p, int kind);  // 0 forward, 1 forward + ring, 2 reverse
+    int launch_paired(const StepParams &p, int kind);   // 0 forward, 1 forward + ring, 2 reverse
+    UnfusedParams unfused_params(const StepParams &p, int kind) const;
+    int paired_lead(int kind) const;
+    int begin_steps();             // before a time loop of step launches
+    int end_steps(int n_steps);    // after it
     void drop_graphs();
     StepParams base_params() const;
     void free_all();
@@ -207,8 +218,14 @@ class Engine {
     struct {
         const int *src_ptr, *src_off, *src_id, *src_cta, *rcv_ptr, *rcv_off, *rcv_id, *rcv_cta;
         const int *rec_off, *ring_off, *ring_cta, *ring_cta_off, *ring_cta_k;
+        const int *rec_cta, *rec_cta_off, *rec_cta_id;  // every receiver grouped by owning block
         int n_src_cells, n_rcv_cells, ncb, nseg;
     } utb_{};
+    // paired kernels: ticket counter (first 256 bytes) and done counts
+    // [max_shots][nseg]
+    void *pair_sync_ = nullptr;
+    size_t pair_sync_bytes_ = 0;
+    int pair_lead_ = 0;
     int n_strips_ = 0, seg_h_ = 64;
     int *derr_ = nullptr;         // device error flag of the bounded waits
     TmaParams *tmap_ = nullptr;   // tensor maps of every field, slot and coefficient

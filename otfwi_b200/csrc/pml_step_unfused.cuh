@@ -80,6 +80,16 @@ __device__ __forceinline__ void pdl_enter()
 }
 
 __device__ __forceinline__ float4 uld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+// P(t) as the A half-step reads it: through the read-only path when another
+// launch wrote it (unfused kernels), from L2 (ld.global.cg, coherent) when
+// P items of the same launch wrote it (paired kernels, pml_step_paired.cuh)
+template <bool COHERENT>
+__device__ __forceinline__ float4 pld4(const float *p)
+{
+    if (COHERENT)
+        return __ldcg(reinterpret_cast<const float4 *>(p));
+    return __ldg(reinterpret_cast<const float4 *>(p));
+}
 __device__ __forceinline__ float4 uld4c(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void ust4(float *p, const float *v)
 {
@@ -275,6 +285,68 @@ __device__ __forceinline__ void a_update(const StepParams &p, bool revert, float
     }
 }
 
+// Forward A half-step of one 4-column segment of rows z0 .. z0+7 of a shot:
+// Ax, Az (t) from P(t) (pld4<COHERENT>) and Ax, Az (t-1).
+template <bool COHERENT>
+__device__ __forceinline__ void a_fwd_segment(const UnfusedParams &U, int shot, int x, int z0)
+{
+    const StepParams &p = U.p;
+    const int64_t so = p.shot_stride * shot;
+    const float *__restrict__ P = p.f0.px_out + so;
+    const float *__restrict__ AXI = p.f0.ax_in + so;
+    const float *__restrict__ AZI = p.f0.az_in + so;
+    float *__restrict__ AXO = p.f0.ax_out + so;
+    float *__restrict__ AZO = p.f0.az_out + so;
+    const int64_t col = x + PAD, pitch = p.pitch;
+    float dmx[4];
+    f4a(uld4(p.dampx + col), dmx);
+    float w[4][8];
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        const float4 v = pld4<COHERENT>(P + (int64_t)(z0 - 3 + k + PAD) * pitch + col);
+        w[0][k] = v.x;
+        w[1][k] = v.y;
+        w[2][k] = v.z;
+        w[3][k] = v.w;
+    }
+    const int nz = min(kURows, p.Z - z0);
+#pragma unroll 2
+    for (int r = 0; r < nz; r++) {
+        const int z = z0 + r;
+        const int64_t o = (int64_t)(z + PAD) * pitch + col;
+        {
+            const float4 v = pld4<COHERENT>(P + o + 4 * pitch);
+            w[0][7] = v.x;
+            w[1][7] = v.y;
+            w[2][7] = v.z;
+            w[3][7] = v.w;
+        }
+        float u[12], ax[4], az[4], nx[4], nzv[4];
+        f4a(pld4<COHERENT>(P + o - 4), u);
+        f4a(pld4<COHERENT>(P + o), u + 4);
+        f4a(pld4<COHERENT>(P + o + 4), u + 8);
+        f4a(uld4(AXI + o), ax);
+        f4a(uld4(AZI + o), az);
+        const float dmz = __ldg(p.dampz + z + PAD);
+        const bool zin = z >= 4 && z < p.Z - 4;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float dx, dz;
+            dstag_n<1>(u + j + 1, &dx);
+            dstag_n<1>(w[j], &dz);
+            a_update(p, false, dmx[j], dmz, dx, dz, ax[j], az[j], zin && x + j >= 4 && x + j < p.X - 4, nx[j],
+                     nzv[j]);
+        }
+        ust4(AXO + o, nx);
+        ust4(AZO + o, nzv);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int k = 0; k < 7; k++)
+                w[j][k] = w[j][k + 1];
+    }
+}
+
 // Forward A half-step: grid (ncb, n_tail + nseg, n_shots); the first n_tail
 // rows of CTAs record the receivers (and the ring) of their shot: first, so
 // that these latency-bound CTAs run beside the stencil CTAs, not after them.
@@ -303,71 +375,16 @@ __global__ void __launch_bounds__(kUThreads, kUAMinBlocks) k_unfused_a_fwd(const
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= p.X)
         return;
-    const int z0 = (blockIdx.y - n_tail) * kURows;
-    const float *__restrict__ AXI = p.f0.ax_in + so;
-    const float *__restrict__ AZI = p.f0.az_in + so;
-    float *__restrict__ AXO = p.f0.ax_out + so;
-    float *__restrict__ AZO = p.f0.az_out + so;
-    const int64_t col = x + PAD, pitch = p.pitch;
-    float dmx[4];
-    f4a(uld4(p.dampx + col), dmx);
-    float w[4][8];
-#pragma unroll
-    for (int k = 0; k < 7; k++) {
-        const float4 v = uld4(P + (int64_t)(z0 - 3 + k + PAD) * pitch + col);
-        w[0][k] = v.x;
-        w[1][k] = v.y;
-        w[2][k] = v.z;
-        w[3][k] = v.w;
-    }
-    const int nz = min(kURows, p.Z - z0);
-#pragma unroll 2
-    for (int r = 0; r < nz; r++) {
-        const int z = z0 + r;
-        const int64_t o = (int64_t)(z + PAD) * pitch + col;
-        {
-            const float4 v = uld4(P + o + 4 * pitch);
-            w[0][7] = v.x;
-            w[1][7] = v.y;
-            w[2][7] = v.z;
-            w[3][7] = v.w;
-        }
-        float u[12], ax[4], az[4], nx[4], nzv[4];
-        f4a(uld4(P + o - 4), u);
-        f4a(uld4(P + o), u + 4);
-        f4a(uld4(P + o + 4), u + 8);
-        f4a(uld4(AXI + o), ax);
-        f4a(uld4(AZI + o), az);
-        const float dmz = __ldg(p.dampz + z + PAD);
-        const bool zin = z >= 4 && z < p.Z - 4;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            float dx, dz;
-            dstag_n<1>(u + j + 1, &dx);
-            dstag_n<1>(w[j], &dz);
-            a_update(p, false, dmx[j], dmz, dx, dz, ax[j], az[j], zin && x + j >= 4 && x + j < p.X - 4, nx[j],
-                     nzv[j]);
-        }
-        ust4(AXO + o, nx);
-        ust4(AZO + o, nzv);
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int k = 0; k < 7; k++)
-                w[j][k] = w[j][k + 1];
-    }
+    a_fwd_segment<false>(U, shot, x, (blockIdx.y - n_tail) * kURows);
 }
 
-// Reverse A half-steps of both sets and the imaging condition: grid (ncb,
-// nseg, n_shots).
-__global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_constant__ UnfusedParams U)
+// Reverse A half-steps of both sets and the imaging condition on one
+// 4-column segment of rows z0 .. z0+7 of a shot (P(t) of both sets read with
+// pld4<COHERENT>).
+template <bool COHERENT>
+__device__ __forceinline__ void a_rev_segment(const UnfusedParams &U, int shot, int x, int z0)
 {
-    pdl_enter();
     const StepParams &p = U.p;
-    const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
-    if (x >= p.X)
-        return;
-    const int shot = blockIdx.z, z0 = blockIdx.y * kURows;
     const int64_t so = p.shot_stride * shot;
     const float *__restrict__ PR = p.f0.px_out + so;
     const float *__restrict__ PA = p.f1.px_out + so;
@@ -381,7 +398,7 @@ __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_consta
     float wr[4][9], wa[4][8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-        const float4 v = uld4(PR + (int64_t)(z0 - 4 + k + PAD) * pitch + col);
+        const float4 v = pld4<COHERENT>(PR + (int64_t)(z0 - 4 + k + PAD) * pitch + col);
         wr[0][k] = v.x;
         wr[1][k] = v.y;
         wr[2][k] = v.z;
@@ -389,7 +406,7 @@ __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_consta
     }
 #pragma unroll
     for (int k = 0; k < 7; k++) {
-        const float4 v = uld4(PA + (int64_t)(z0 - 3 + k + PAD) * pitch + col);
+        const float4 v = pld4<COHERENT>(PA + (int64_t)(z0 - 3 + k + PAD) * pitch + col);
         wa[0][k] = v.x;
         wa[1][k] = v.y;
         wa[2][k] = v.z;
@@ -401,12 +418,12 @@ __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_consta
         const int64_t o = (int64_t)(z + PAD) * pitch + col;
         const bool zin = z >= 4 && z < p.Z - 4;
         {
-            const float4 v = uld4(PR + o + 4 * pitch);
+            const float4 v = pld4<COHERENT>(PR + o + 4 * pitch);
             wr[0][8] = v.x;
             wr[1][8] = v.y;
             wr[2][8] = v.z;
             wr[3][8] = v.w;
-            const float4 a = uld4(PA + o + 4 * pitch);
+            const float4 a = pld4<COHERENT>(PA + o + 4 * pitch);
             wa[0][7] = a.x;
             wa[1][7] = a.y;
             wa[2][7] = a.z;
@@ -416,9 +433,9 @@ __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_consta
         {
             // reconstruction: reverted A update and the Laplacian of P_rec(t)
             float u[12], ax[4], az[4], nx[4], nzv[4];
-            f4a(uld4(PR + o - 4), u);
-            f4a(uld4(PR + o), u + 4);
-            f4a(uld4(PR + o + 4), u + 8);
+            f4a(pld4<COHERENT>(PR + o - 4), u);
+            f4a(pld4<COHERENT>(PR + o), u + 4);
+            f4a(pld4<COHERENT>(PR + o + 4), u + 8);
             f4a(uld4(p.f0.ax_in + so + o), ax);
             f4a(uld4(p.f0.az_in + so + o), az);
 #pragma unroll
@@ -437,9 +454,9 @@ __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_consta
         {
             // adjoint: damped A update and the imaging condition
             float u[12], ax[4], az[4], nx[4], nzv[4], g[4];
-            f4a(uld4(PA + o - 4), u);
-            f4a(uld4(PA + o), u + 4);
-            f4a(uld4(PA + o + 4), u + 8);
+            f4a(pld4<COHERENT>(PA + o - 4), u);
+            f4a(pld4<COHERENT>(PA + o), u + 4);
+            f4a(pld4<COHERENT>(PA + o + 4), u + 8);
             f4a(uld4(p.f1.ax_in + so + o), ax);
             f4a(uld4(p.f1.az_in + so + o), az);
             f4a(uld4c(p.grad + so + o), g);
@@ -466,6 +483,17 @@ __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_consta
                 wa[j][k] = wa[j][k + 1];
         }
     }
+}
+
+// Reverse A half-steps of both sets and the imaging condition: grid (ncb,
+// nseg, n_shots).
+__global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_constant__ UnfusedParams U)
+{
+    pdl_enter();
+    const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
+    if (x >= U.p.X)
+        return;
+    a_rev_segment<false>(U, blockIdx.z, x, blockIdx.y * kURows);
 }
 
 }  // namespace otf
