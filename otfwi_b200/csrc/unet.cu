@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "otf_common.cuh"
+#include "tma.cuh"
 
 namespace otf {
 namespace unet {
@@ -209,6 +210,8 @@ struct WgradArgs {
     float *dw;           // [9][cout][cin] FP32, accumulated
     int N, H, W;
 };
+
+#include "unet_umma.cuh"
 
 constexpr int WG_DZ_LD = TW * TH + 8;   // 136 BF16 per output channel row
 constexpr int WG_X_LD = HHT * HWD + 4;  // 184 BF16 per input channel row
@@ -556,6 +559,8 @@ __global__ void k_pack_weights(const float *__restrict__ w, int cout, int cin, b
 using namespace otf::unet;
 
 namespace {
+int g_use_umma = 1;
+bool use_umma() { return g_use_umma != 0; }
 inline unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 int launch_status()
 {
@@ -598,9 +603,54 @@ int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1
     a.N = N;
     a.H = H;
     a.W = W;
+    if (use_umma()) {
+        // tensor-core (tcgen05) path: every output channel of a pixel tile in
+        // one CTA where cout <= 256, else blocks of 256 / 128 / 64 / 32
+        int nb = cout;
+        for (int c : {256, 128, 64, 32})
+            if (nb > 256 && cout % c == 0)
+                nb = c;
+        const int tiles = ((W + umma::TWU - 1) / umma::TWU) * ((H + umma::THU - 1) / umma::THU) * N;
+        const dim3 grid((unsigned)tiles, (unsigned)(cout / nb));
+        if (nb > 128) {
+            const int smem = umma_smem_bytes(nb, 2);
+            OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_umma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            k_conv3x3_umma<2><<<grid, 128, smem, (cudaStream_t)stream>>>(a, nb);
+        } else {
+            const int smem = umma_smem_bytes(nb, 3);
+            OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_umma<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            k_conv3x3_umma<3><<<grid, 128, smem, (cudaStream_t)stream>>>(a, nb);
+        }
+        return launch_status();
+    }
     const int tiles = ((W + TW - 1) / TW) * ((H + TH - 1) / TH) * N;
     k_conv3x3<<<dim3((unsigned)tiles, (unsigned)(cout / BN)), 128, 0, (cudaStream_t)stream>>>(a);
     return launch_status();
+}
+
+/* Tensor-core path of the 3x3 convolution and its weight gradient: 1 =
+ * tcgen05 (default), 0 = the warp-level mma.sync kernels; returns the
+ * previous setting. */
+int otf_unet_set_umma(int on)
+{
+    const int prev = g_use_umma;
+    g_use_umma = on ? 1 : 0;
+    return prev;
+}
+
+/* Error bits recorded by the U-Net tensor-core kernels since the last call
+ * (1 = a bounded wait timed out; the results of that launch are invalid);
+ * cleared by the call. Returns -1 if the flag cannot be read. */
+int otf_unet_status(void)
+{
+    int h = 0;
+    const int zero = 0;
+    if (cudaMemcpyFromSymbol(&h, g_unet_err, sizeof(int)) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_unet_err, &zero, sizeof(int)) != cudaSuccess) {
+        otf::set_error_msg(5, "unet status: flag read failed");
+        return -1;
+    }
+    return h;
 }
 
 int otf_unet_conv3x3_wgrad(const void *src0, int c0, const void *src1, int c1, int up1, const void *dz,
@@ -620,6 +670,33 @@ int otf_unet_conv3x3_wgrad(const void *src0, int c0, const void *src1, int c1, i
     a.N = N;
     a.H = H;
     a.W = W;
+    if (use_umma()) {
+        // tensor-core path: 128 output channels x 32 (or 16) input channels x
+        // 9 taps per CTA, the pixels split into slab ranges so that about one
+        // CTA per SM (two with 16 input channels) runs
+        const int cin = c0 + c1;
+        const int nw = cin % 32 == 0 ? 32 : 16;
+        const int n_slabs = ((W + umma::TWU - 1) / umma::TWU) * ((H + umma::THU - 1) / umma::THU) * N;
+        const int gy = (cout + 127) / 128, gz = cin / nw;
+        const int target = (sm_count > 0 ? sm_count : 148) * (nw == 32 ? 1 : 2);
+        int gx = target / (gy * gz);
+        gx = gx < 1 ? 1 : (gx > n_slabs ? n_slabs : gx);
+        const int spc = (n_slabs + gx - 1) / gx;
+        gx = (n_slabs + spc - 1) / spc;
+        const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)gz);
+        if (nw == 32) {
+            const int smem = umma_wg_smem_bytes(32, 3);
+            OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_wgrad_umma<32, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          smem));
+            k_conv3x3_wgrad_umma<32, 3><<<grid, 128, smem, (cudaStream_t)stream>>>(a, spc);
+        } else {
+            const int smem = umma_wg_smem_bytes(16, 3);
+            OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_wgrad_umma<16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          smem));
+            k_conv3x3_wgrad_umma<16, 3><<<grid, 128, smem, (cudaStream_t)stream>>>(a, spc);
+        }
+        return launch_status();
+    }
     const int slabs = ((W + TW - 1) / TW) * ((H + TH - 1) / TH) * N;
     const int tiles = (cout / BN) * ((c0 + c1) / KC);
     const int target = 4 * (sm_count > 0 ? sm_count : 148);

@@ -1,0 +1,413 @@
+// 3x3 convolution on the 5th-generation tensor cores (tcgen05 / UMMA) for
+// the preconditioner U-Net: an implicit GEMM with
+//
+//   M = 128 output pixels (a tile 8 wide x 16 tall of one image),
+//   N = every output channel of the CTA (cout, or 256 of them, <= 256),
+//   K = 9 taps x the input channels, taken 16 channels (one MMA K) at a time.
+//
+// Per 16-channel chunk the CTA stages, with cp.async (zero fill at the image
+// border; the second input upsampled on load as in k_conv3x3), the input halo
+// (18 x 10 pixels) as two 8-channel planes [pixel][8 channels], and the
+// chunk's weights of every tap as [tap][plane][cout][8 channels]. Both are
+// the no-swizzle K-major canonical UMMA layout: a core matrix is 8 rows of 16
+// bytes. For tap (dy, dx) the A operand is the halo shifted by (dy, dx):
+// row m of A (output pixel oy = m / 8, ox = m % 8) is halo pixel (oy + dy) *
+// 10 + ox + dx, so 8 consecutive rows are 8 consecutive halo pixels (one core
+// matrix), consecutive core matrices are one halo row (160 bytes) apart, and
+// the second K half is the other plane: one descriptor per tap, no copy. One
+// thread issues the 9 MMAs of a chunk (tcgen05.mma kind::f16, BF16 inputs,
+// FP32 accumulators in tensor memory, 128 lanes x N columns) and commits
+// them to the stage's mbarrier; the stage is refilled once that barrier
+// completes. The epilogue reads the accumulators with tcgen05.ld (warp w owns
+// lanes 32w .. 32w+31, i.e. tile rows 4w .. 4w+3), adds the bias, applies the
+// ReLU and the optional masks, and writes BF16 to the split outputs as
+// k_conv3x3 does.
+//
+// Every mbarrier wait is bounded (tma.cuh: 0.5 s); on expiry the kernel sets
+// the error flag, skips its remaining MMAs and epilogue, waits (bounded) for
+// the MMAs it issued, frees its tensor memory and exits.
+#pragma once
+// included inside namespace otf::unet by unet.cu, after tma.cuh
+
+namespace umma {
+
+constexpr int TWU = 8, THU = 16;              // output tile (x, y): 128 pixels
+constexpr int HWU = TWU + 2, HHU = THU + 2;   // halo 10 x 18
+constexpr int HPIX = HWU * HHU;               // 180 halo pixels
+constexpr int PLANE_A = HPIX * 16;            // bytes of one 8-channel plane of the halo
+constexpr int A_BYTES = 2 * PLANE_A;          // 5760
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    // start >> 4 [0,14), LBO >> 4 [16,30), SBO >> 4 [32,46), version 1 [46,48),
+    // base offset 0, no swizzle (layout type 0 in [61,64))
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: FP32 accumulators, BF16 A and B, both
+// K-major, M = 128, N.
+__host__ __device__ constexpr uint32_t instr_desc_bf16(int n)
+{
+    return (1u << 4)                          // D format F32
+           | (1u << 7)                        // A format BF16
+           | (1u << 10)                       // B format BF16
+           | ((uint32_t)(n >> 3) << 17)       // N / 8
+           | ((uint32_t)(128 >> 4) << 24);    // M / 16
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, bool acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"((uint32_t)acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     otf::smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(otf::smem_u32(slot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v)
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,"
+        "%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+          "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+          "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++)
+        v[i] = __uint_as_float(r[i]);
+}
+
+}  // namespace umma
+
+// dynamic shared memory of the UMMA conv: NST stages of (halo + weights),
+// the stage barriers and the tensor-memory address slot
+__host__ __device__ constexpr int umma_stage_bytes(int n) { return umma::A_BYTES + 9 * 2 * n * 16; }
+__host__ __device__ constexpr int umma_smem_bytes(int n, int nst) { return nst * umma_stage_bytes(n) + 128; }
+
+__device__ int g_unet_err;  // set by a timed-out wait of a U-Net tensor-core kernel
+
+// One CTA: 128 output pixels (8 x 16) of one image x N output channels
+// (blockIdx.y selects the block of N channels); 4 warps.
+template <int NST>
+__global__ void __launch_bounds__(128) k_conv3x3_umma(ConvArgs a, int N)
+{
+    extern __shared__ __align__(128) unsigned char smu[];
+    const int sb = umma_stage_bytes(N);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smu + NST * sb);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + NST + 1);
+    const int tiles_x = (a.W + umma::TWU - 1) / umma::TWU, tiles_y = (a.H + umma::THU - 1) / umma::THU;
+    int bidx = blockIdx.x;
+    const int n = bidx / (tiles_x * tiles_y);
+    bidx -= n * tiles_x * tiles_y;
+    const int ty = bidx / tiles_x, tx = bidx - ty * tiles_x;
+    const int y0 = ty * umma::THU, x0 = tx * umma::TWU, co0 = blockIdx.y * N;
+    const int cin = a.c0 + a.c1, nk = cin / KC;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t ncols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s <= NST; s++)
+            otf::mbar_init(&bar[s], 1);
+        otf::fence_barrier_init();
+    }
+    if (warp == 0)
+        umma::tmem_alloc(tslot, ncols);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    const uint32_t idesc = umma::instr_desc_bf16(N);
+
+    auto load = [&](int kc, unsigned char *st) {
+        uint32_t *sa = reinterpret_cast<uint32_t *>(st);
+        for (int i = threadIdx.x; i < umma::HPIX * 2; i += 128) {
+            const int px = i >> 1, half = i & 1;
+            const int hy = px / umma::HWU, hx = px - hy * umma::HWU;
+            const int gy = y0 + hy - 1, gx = x0 + hx - 1;
+            const bool ok = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
+            const void *src = ok ? (const void *)in_ptr(a, n, gy, gx, kc * KC + half * 8) : (const void *)a.w;
+            cp_async16(sa + (half * umma::PLANE_A + px * 16) / 4, src, ok ? 16 : 0);
+        }
+        uint32_t *sw = reinterpret_cast<uint32_t *>(st + umma::A_BYTES);
+        for (int i = threadIdx.x; i < 9 * N * 2; i += 128) {
+            const int row = i >> 1, half = i & 1;
+            const int tap = row / N, co = row - tap * N;
+            cp_async16(sw + ((tap * 2 + half) * N + co) * 4,
+                       a.w + (int64_t)(tap * a.cout + co0 + co) * cin + kc * KC + half * 8, 16);
+        }
+    };
+
+    bool ok = true;
+    load(0, smu);
+    cp_commit();
+    for (int kc = 0; kc < nk; kc++) {
+        const int s = kc % NST;
+        if (kc + 1 < nk) {
+            const int s1 = (kc + 1) % NST;
+            // the stage's previous chunk (kc + 1 - NST) must have been consumed
+            if (kc + 1 >= NST && ok)
+                ok = otf::mbar_wait(&bar[s1], (uint32_t)(((kc + 1) / NST - 1) & 1), &g_unet_err);
+            load(kc + 1, smu + s1 * sb);
+        }
+        cp_commit();
+        cp_wait<1>();
+        umma::fence_proxy_async();  // cp.async writes -> visible to the tensor cores
+        __syncthreads();
+        if (threadIdx.x == 0 && ok) {
+            umma::fence_after_sync();
+            const uint32_t abase = otf::smem_u32(smu + s * sb);
+            const uint32_t bbase = abase + umma::A_BYTES;
+#pragma unroll
+            for (int tap = 0; tap < 9; tap++) {
+                const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+                const uint64_t ad = umma::smem_desc(abase + (dy * umma::HWU + dx) * 16, umma::PLANE_A,
+                                                    umma::HWU * 16);
+                const uint64_t bd = umma::smem_desc(bbase + tap * 2 * N * 16, N * 16, 128);
+                umma::mma_bf16(tmem, ad, bd, idesc, kc > 0 || tap > 0);
+            }
+            umma::mma_commit(&bar[s]);
+        }
+        __syncthreads();
+    }
+    // all MMAs complete: one more commit (tracks every MMA issued before it)
+    if (threadIdx.x == 0)
+        umma::mma_commit(&bar[NST]);
+    const bool done = otf::mbar_wait(&bar[NST], 0, &g_unet_err);
+    ok = ok && done;
+    umma::fence_after_sync();
+
+    if (ok) {
+        const int m = warp * 32 + lane;
+        const int y = y0 + m / umma::TWU, x = x0 + (m % umma::TWU);
+        const bool inside = y < a.H && x < a.W;
+        const int64_t pix = ((int64_t)n * a.H + y) * a.W + x;
+        for (int c0 = 0; c0 < N; c0 += 32) {
+            float v[32];
+            umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (!inside)
+                continue;
+#pragma unroll
+            for (int j = 0; j < 32; j += 2) {
+                const int co = co0 + c0 + j;
+                float v0 = v[j], v1 = v[j + 1];
+                if (a.bias) {
+                    v0 += a.bias[co];
+                    v1 += a.bias[co + 1];
+                }
+                if (a.relu) {
+                    v0 = fmaxf(v0, 0.f);
+                    v1 = fmaxf(v1, 0.f);
+                }
+                const bool lo = co < a.split;
+                bf16 *dst = lo ? a.dst0 : a.dst1;
+                const bf16 *mask = lo ? a.mask0 : a.mask1;
+                const int cc = lo ? a.split : a.cout - a.split, ci = lo ? co : co - a.split;
+                if (mask) {
+                    const bf162 mk = *reinterpret_cast<const bf162 *>(mask + pix * cc + ci);
+                    if (!(__low2float(mk) > 0.f))
+                        v0 = 0.f;
+                    if (!(__high2float(mk) > 0.f))
+                        v1 = 0.f;
+                }
+                *reinterpret_cast<bf162 *>(dst + pix * cc + ci) = __floats2bfloat162_rn(v0, v1);
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(tmem, ncols);
+    }
+}
+
+// Weight gradient on the tcgen05 tensor cores: for each tap,
+//
+//   D_tap[co][ci] += sum over pixels p of dz[p][co] * x[p + tap][ci],
+//
+// an implicit GEMM with M = 128 output channels (rows beyond cout staged as
+// zeros), N = 32 input channels (16 when the layer has 16), K = pixels, 16
+// (two tile rows) per MMA; the 9 taps' accumulators sit side by side in
+// tensor memory (9 x N columns). Both operands are MN-major (channels
+// contiguous, as the activations are stored): per 128-pixel slab (8 x 16) the
+// CTA stages dz as [co / 8][pixel][8 co] and the input halo as [ci / 8][halo
+// pixel][8 ci], the no-swizzle MN-major canonical UMMA layout (a core matrix
+// is 8 channels x 8 pixels, 128 contiguous bytes). For tap (dy, dx) and K
+// step s the B operand starts at halo pixel (2s + dy) * 10 + dx: eight
+// pixels of one tile row are eight consecutive halo pixels, the next tile row
+// is one halo row (160 bytes) further. A CTA walks a range of slabs, then adds
+// its 9 x 128 x N partial sums to dw with FP32 atomics (the mma.sync kernel's
+// reduction). Bounded waits as the forward kernel.
+__host__ __device__ constexpr int umma_wg_stage_bytes(int nw) { return 128 * 256 + (nw / 8) * umma::PLANE_A; }
+__host__ __device__ constexpr int umma_wg_smem_bytes(int nw, int nst) { return nst * umma_wg_stage_bytes(nw) + 128; }
+
+__host__ __device__ constexpr uint32_t instr_desc_bf16_mn(int n)
+{
+    return umma::instr_desc_bf16(n) | (1u << 15) | (1u << 16);  // A and B MN-major
+}
+
+template <int NW, int NST>
+__global__ void __launch_bounds__(128) k_conv3x3_wgrad_umma(WgradArgs a, int slabs_per_cta)
+{
+    extern __shared__ __align__(128) unsigned char smu[];
+    constexpr int SB = umma_wg_stage_bytes(NW);
+    constexpr uint32_t NCOLS = 9 * NW <= 256 ? 256u : 512u;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smu + NST * SB);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + NST + 1);
+    const int co0 = blockIdx.y * 128, ci0 = blockIdx.z * NW;
+    const int cin = a.c0 + a.c1;
+    const int tiles_x = (a.W + umma::TWU - 1) / umma::TWU, tiles_y = (a.H + umma::THU - 1) / umma::THU;
+    const int n_slabs = tiles_x * tiles_y * a.N;
+    const int s_begin = blockIdx.x * slabs_per_cta, s_end = min(n_slabs, s_begin + slabs_per_cta);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    ConvArgs ca{};
+    ca.src0 = a.src0;
+    ca.src1 = a.src1;
+    ca.c0 = a.c0;
+    ca.c1 = a.c1;
+    ca.up1 = a.up1;
+    ca.N = a.N;
+    ca.H = a.H;
+    ca.W = a.W;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s <= NST; s++)
+            otf::mbar_init(&bar[s], 1);
+        otf::fence_barrier_init();
+    }
+    if (warp == 0)
+        umma::tmem_alloc(tslot, NCOLS);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    const uint32_t idesc = instr_desc_bf16_mn(NW);
+
+    auto load = [&](int slab, unsigned char *st) {
+        int b = slab;
+        const int n = b / (tiles_x * tiles_y);
+        b -= n * tiles_x * tiles_y;
+        const int ty = b / tiles_x, tx = b - ty * tiles_x;
+        const int y0 = ty * umma::THU, x0 = tx * umma::TWU;
+        uint32_t *sd = reinterpret_cast<uint32_t *>(st);
+        // dz: 128 pixels x 128 output channels, 8 channels per copy
+        for (int i = threadIdx.x; i < 128 * 16; i += 128) {
+            const int g = i >> 7, px = i & 127;  // channel group, pixel (oy * 8 + ox)
+            const int y = y0 + (px >> 3), x = x0 + (px & 7), co = co0 + g * 8;
+            const bool ok = y < a.H && x < a.W && co < a.cout;
+            const void *src = ok ? (const void *)(a.dz + (((int64_t)n * a.H + y) * a.W + x) * a.cout + co)
+                                 : (const void *)a.dz;
+            cp_async16(sd + (g * 128 + px) * 4, src, ok ? 16 : 0);
+        }
+        uint32_t *sx = reinterpret_cast<uint32_t *>(st + 128 * 256);
+        for (int i = threadIdx.x; i < umma::HPIX * (NW / 8); i += 128) {
+            const int g = i / umma::HPIX, px = i - g * umma::HPIX;
+            const int hy = px / umma::HWU, hx = px - hy * umma::HWU;
+            const int gy = y0 + hy - 1, gx = x0 + hx - 1;
+            const bool ok = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
+            const void *src = ok ? (const void *)in_ptr(ca, n, gy, gx, ci0 + g * 8) : (const void *)a.dz;
+            cp_async16(sx + (g * umma::PLANE_A + px * 16) / 4, src, ok ? 16 : 0);
+        }
+    };
+
+    bool ok = true;
+    const int nsl = s_end - s_begin;
+    if (nsl > 0) {
+        load(s_begin, smu);
+        cp_commit();
+    }
+    for (int k = 0; k < nsl; k++) {
+        const int s = k % NST;
+        if (k + 1 < nsl) {
+            const int s1 = (k + 1) % NST;
+            if (k + 1 >= NST && ok)
+                ok = otf::mbar_wait(&bar[s1], (uint32_t)(((k + 1) / NST - 1) & 1), &g_unet_err);
+            load(s_begin + k + 1, smu + s1 * SB);
+        }
+        cp_commit();
+        cp_wait<1>();
+        umma::fence_proxy_async();
+        __syncthreads();
+        if (threadIdx.x == 0 && ok) {
+            umma::fence_after_sync();
+            const uint32_t abase = otf::smem_u32(smu + s * SB);
+            const uint32_t bbase = abase + 128 * 256;
+#pragma unroll 1
+            for (int tap = 0; tap < 9; tap++) {
+                const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+#pragma unroll
+                for (int ks = 0; ks < 8; ks++) {
+                    // A: channel groups 2048 bytes apart, K groups (tile rows) 128 bytes apart
+                    const uint64_t ad = umma::smem_desc(abase + ks * 256, 128, 128 * 16);
+                    // B: channel groups one plane apart, K groups (tile rows) one halo row apart
+                    const uint64_t bd = umma::smem_desc(bbase + ((2 * ks + dy) * umma::HWU + dx) * 16,
+                                                        umma::HWU * 16, umma::PLANE_A);
+                    umma::mma_bf16(tmem + (uint32_t)(tap * NW), ad, bd, idesc, k > 0 || ks > 0);
+                }
+            }
+            umma::mma_commit(&bar[s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        umma::mma_commit(&bar[NST]);
+    const bool done = otf::mbar_wait(&bar[NST], 0, &g_unet_err);
+    ok = ok && done;
+    umma::fence_after_sync();
+
+    if (ok && nsl > 0) {
+        const int co = co0 + warp * 32 + lane;  // TMEM lane = output channel row
+        for (int tap = 0; tap < 9; tap++) {
+            for (int c = 0; c < NW; c += 16) {
+                // 32 columns from tap * NW + c (inside the allocation); the
+                // first 16 are this (tap, c .. c+15)
+                float v[32];
+                umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(tap * NW + c), v);
+                if (co < a.cout) {
+                    float *d = a.dw + ((int64_t)tap * a.cout + co) * cin + ci0 + c;
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        atomicAdd(d + j, v[j]);
+                }
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(tmem, NCOLS);
+    }
+}

@@ -43,6 +43,8 @@ def _declare(L):
         "otf_unet_mse": [v, v, v, ll, f, v, v, v],
         "otf_unet_adam": [v, v, v, v, ll, f, f, f, f, i, f, v],
         "otf_unet_pack_weights": [v, i, i, v, v, v],
+        "otf_unet_set_umma": [i],
+        "otf_unet_status": [],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -321,8 +323,10 @@ def _bench(argv=None):
     ap.add_argument("--n", type=int, default=16)
     ap.add_argument("--hw", type=int, default=256)
     ap.add_argument("--iters", type=int, default=10)
+    ap.add_argument("--legacy", action="store_true", help="warp-level mma.sync convolutions instead of tcgen05")
     a = ap.parse_args(argv)
     net = UNet(base=32)
+    net.L.otf_unet_set_umma(0 if a.legacy else 1)
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
     x = torch.randn(a.n, a.hw, a.hw, 3, device="cuda", generator=g)
@@ -349,8 +353,10 @@ def _bench(argv=None):
     for name, cin, cout in net.layers:
         lvl = {"enc1": 0, "dec1": 0, "enc2": 1, "dec2": 1, "enc3": 2, "dec3": 2, "bota": 3, "botb": 3}[name[:4]]
         flop += 2.0 * 9 * cin * cout * a.n * (a.hw >> lvl) ** 2
-    print(json.dumps({"n": a.n, "hw": a.hw, "forward_ms": f_ms, "forward_tflops": flop / f_ms / 1e9,
-                      "train_step_ms": s_ms, "train_tflops": 3 * flop / s_ms / 1e9}))
+    status = int(net.L.otf_unet_status())
+    print(json.dumps({"n": a.n, "hw": a.hw, "conv": "mma.sync" if a.legacy else "tcgen05",
+                      "forward_ms": f_ms, "forward_tflops": flop / f_ms / 1e9,
+                      "train_step_ms": s_ms, "train_tflops": 3 * flop / s_ms / 1e9, "device_status": status}))
 
 
 if __name__ == "__main__":
