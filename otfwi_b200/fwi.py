@@ -224,7 +224,10 @@ def descent(prob, c0, proposer=None, alpha0=None, on_step=None, on_iter=None, pr
     torch = prob.torch
     c = prob.clip(torch.as_tensor(np.asarray(c0, np.float32)).cuda().clone())
     h = History()
-    torch.cuda.synchronize()
+    # the library's calls wait for their own stream; the model updates run on
+    # this thread's torch stream: waiting for that one times an iterate
+    # without stalling inversions that other threads run concurrently
+    torch.cuda.current_stream().synchronize()
     t0 = time.perf_counter()
     evals_total = 0.0
     c_ref = float(c.mean().item())
@@ -266,7 +269,7 @@ def descent(prob, c0, proposer=None, alpha0=None, on_step=None, on_iter=None, pr
                     continue
                 c = prob.clip(c + a * d)
                 alpha = a
-            torch.cuda.synchronize()
+            torch.cuda.current_stream().synchronize()
             h.t.append(time.perf_counter() - t0)
             h.misfit.append(J_new)
             h.rms.append(prob.rms(c))

@@ -94,41 +94,79 @@ def _bands(f_lo, f_hi, iters):
     return [fwi.Band(f_lo, iters), fwi.Band(f_hi, iters)]
 
 
+def _plain_run(r, seed0, X, Z, T, n_elem, pitch, n_src, iters, bands_hz, misfit):
+    """One plain FWI run of the training set: its (features, target) pairs
+    (FP16, on the GPU), the gradient mask and the run's statistics."""
+    rng = np.random.default_rng(seed0 + r)
+    sc = defect_scenario(X, Z, T, seed0 + r, n_elem, pitch, int(rng.integers(3, 9)), n_src=n_src)
+    prob = fwi.Problem(sc, _bands(bands_hz[0], bands_hz[1], iters), misfit=misfit)
+    feats, models, pending = [], [], {}
+
+    def on_step(b, it, c, g, J0):
+        pending["p"] = (features(prob, b, c, g)[0].half(), c.clone())
+
+    def on_iter(b, it, c_new, g, J0, J_new):
+        f, ck = pending.pop("p")
+        feats.append(f)
+        models.append(ck)
+
+    c_fin, h = fwi.descent(prob, sc.c_start, on_step=on_step, on_iter=on_iter)
+    ys = [((c_fin - ck) / SPAN * prob.gmask).half() for ck in models]
+    stat = {"seed": seed0 + r, "rms0": h.rms[0], "rms_final": h.rms[-1], "iters": len(h.rms) - 1,
+            "wall_s": h.t[-1], "pairs": len(feats)}
+    gmask = prob.gmask.clone()
+    for sb in prob._batches.values():
+        sb.close()
+    return feats, ys, gmask, stat
+
+
 def generate(n_runs, seed0=1000, X=256, Z=256, T=1500, n_elem=32, pitch=6, n_src=16, iters=8,
-             bands_hz=(2.5e6, 5e6), misfit="wasserstein", log=None):
+             bands_hz=(2.5e6, 5e6), misfit="wasserstein", log=None, workers=1):
     """Training pairs from n_runs plain FWI runs: (inputs [M, Z, X, 3],
-    targets [M, Z, X], weight [Z, X]) on the GPU, and per-run statistics."""
+    targets [M, Z, X], weight [Z, X]) on the GPU, and per-run statistics.
+
+    ``workers`` > 1 runs that many inversions at once, each in its own host
+    thread with its own CUDA streams (the library's calls release the
+    interpreter lock while they wait): one small inversion leaves most of the
+    GPU idle between its short launches, several fill it. Pairs are returned
+    in run order whatever the worker count."""
+    import threading
     import torch
-    xs, ys, stats = [], [], []
-    weight = None
+    from concurrent.futures import ThreadPoolExecutor
     t0 = time.perf_counter()
-    for r in range(n_runs):
-        rng = np.random.default_rng(seed0 + r)
-        sc = defect_scenario(X, Z, T, seed0 + r, n_elem, pitch, int(rng.integers(3, 9)), n_src=n_src)
-        prob = fwi.Problem(sc, _bands(bands_hz[0], bands_hz[1], iters), misfit=misfit)
-        feats, models, pending = [], [], {}
+    results = [None] * n_runs
+    lock = threading.Lock()
+    dev = torch.cuda.current_device()
+    args = (seed0, X, Z, T, n_elem, pitch, n_src, iters, bands_hz, misfit)
 
-        def on_step(b, it, c, g, J0, prob=prob):
-            pending["p"] = (features(prob, b, c, g)[0].half(), c.clone())
-
-        def on_iter(b, it, c_new, g, J0, J_new):
-            f, ck = pending.pop("p")
-            feats.append(f)
-            models.append(ck)
-
-        c_fin, h = fwi.descent(prob, sc.c_start, on_step=on_step, on_iter=on_iter)
-        for f, ck in zip(feats, models):
-            xs.append(f)
-            ys.append(((c_fin - ck) / SPAN * prob.gmask).half())
-        if weight is None:
-            weight = prob.gmask.clone()
-        stats.append({"seed": seed0 + r, "rms0": h.rms[0], "rms_final": h.rms[-1], "iters": len(h.rms) - 1,
-                      "wall_s": h.t[-1]})
+    def note(r):
         if log:
-            log(f"run {r}: rms {h.rms[0]:.1f} -> {h.rms[-1]:.1f} m/s in {h.t[-1]:.2f} s "
-                f"({len(feats)} pairs, {time.perf_counter() - t0:.0f} s total)")
-        del prob
-    return torch.stack(xs), torch.stack(ys), weight, stats
+            st = results[r][3]
+            with lock:
+                log(f"run {r}: rms {st['rms0']:.1f} -> {st['rms_final']:.1f} m/s in {st['wall_s']:.2f} s "
+                    f"({st['pairs']} pairs, {time.perf_counter() - t0:.0f} s total)")
+
+    def work(w):
+        torch.cuda.set_device(dev)
+        with torch.cuda.stream(torch.cuda.Stream()):
+            for r in range(w, n_runs, workers):
+                out = _plain_run(r, *args)
+                torch.cuda.current_stream().synchronize()
+                results[r] = out
+                note(r)
+
+    if workers <= 1:
+        for r in range(n_runs):
+            results[r] = _plain_run(r, *args)
+            note(r)
+    else:
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            for f in [ex.submit(work, w) for w in range(workers)]:
+                f.result()
+        torch.cuda.synchronize()
+    xs = [x for res in results for x in res[0]]
+    ys = [y for res in results for y in res[1]]
+    return torch.stack(xs), torch.stack(ys), results[0][2], [res[3] for res in results]
 
 
 def train(net, X, Y, weight, steps=4000, batch=16, lr=1e-3, seed=0, log=None, group=None):
@@ -176,6 +214,44 @@ def train(net, X, Y, weight, steps=4000, batch=16, lr=1e-3, seed=0, log=None, gr
     return [float(l.item()) for l in losses]
 
 
+def validation_loss(net, X, Y, weight, batch=16):
+    """Weighted MSE of the network over held-out pairs (no flips, forward
+    only), normalised as the training loss is."""
+    M = X.shape[0]
+    tot, n = 0.0, 0
+    for i in range(0, M, batch):
+        xb = X[i:i + batch].float().contiguous()
+        yb = Y[i:i + batch].float().contiguous()
+        k = xb.shape[0]
+        wb = weight[None].expand(k, -1, -1).contiguous()
+        net.forward(xb)
+        loss = net.loss_grad(yb, wb, inv_norm=1.0 / float(wb.sum().item()))
+        tot += float(loss.item()) * k
+        n += k
+    return tot / max(n, 1)
+
+
+def learning_curve(X, Y, w, stats, n_val, sizes, steps, batch, lr, log=None):
+    """Validation loss on the pairs of the last n_val runs for networks
+    trained (same seed, steps, batch, lr) on the pairs of the first k runs,
+    for each k in sizes: whether more plain-FWI runs still help."""
+    from .unet import UNet
+    ends = np.cumsum([0] + [st["pairs"] for st in stats])
+    n_train = len(stats) - n_val
+    Xv, Yv = X[ends[n_train]:], Y[ends[n_train]:]
+    out = []
+    for k in sizes:
+        k = min(int(k), n_train)
+        net = UNet(base=32, in_ch=3, seed=0)
+        losses = train(net, X[:ends[k]], Y[:ends[k]], w, steps=steps, batch=batch, lr=lr)
+        vl = validation_loss(net, Xv, Yv, w)
+        out.append({"runs": k, "pairs": int(ends[k]), "train_loss_last_100": float(np.mean(losses[-100:])),
+                    "validation_loss": vl})
+        if log:
+            log(f"learning curve: {k} runs ({int(ends[k])} pairs): validation loss {vl:.5f}")
+    return out
+
+
 def evaluate(net, X=512, Z=512, T=4000, n_elem=64, pitch=6, n_src=64, iters=15, seed=7, n_def=8,
              bands_hz=(2.5e6, 5e6), misfit="wasserstein", log=None):
     """Plain vs learned FWI on one seeded model: time for the learned method
@@ -217,6 +293,10 @@ def evaluate(net, X=512, Z=512, T=4000, n_elem=64, pitch=6, n_src=64, iters=15, 
 def main(argv=None):
     ap = argparse.ArgumentParser(description="learned-preconditioned FWI: data, training, evaluation")
     ap.add_argument("--runs", type=int, default=256, help="plain FWI runs that generate training pairs")
+    ap.add_argument("--workers", type=int, default=1, help="plain FWI runs in flight at once (host threads)")
+    ap.add_argument("--val-runs", type=int, default=0,
+                    help="further plain runs held out for a learning curve (validation loss only)")
+    ap.add_argument("--curve", default="", help="comma-separated training-set sizes (runs) of the learning curve")
     ap.add_argument("--train-iters", type=int, default=10, help="plain iterations per band in data runs")
     ap.add_argument("--steps", type=int, default=4000, help="training steps")
     ap.add_argument("--batch", type=int, default=16)
@@ -239,8 +319,17 @@ def main(argv=None):
     rep = {}
     if not a.skip_train:
         t0 = time.perf_counter()
-        X, Y, w, stats = generate(a.runs, iters=a.train_iters, log=log)
-        rep["data"] = {"runs": a.runs, "pairs": int(X.shape[0]), "wall_s": time.perf_counter() - t0,
+        X, Y, w, stats = generate(a.runs + a.val_runs, iters=a.train_iters, log=log, workers=a.workers)
+        data_s = time.perf_counter() - t0
+        if a.curve and a.val_runs:
+            rep["learning_curve"] = learning_curve(X, Y, w, stats, a.val_runs,
+                                                   [int(v) for v in a.curve.split(",")], a.steps, a.batch,
+                                                   a.lr, log=log)
+        if a.val_runs:
+            n_keep = int(np.sum([st["pairs"] for st in stats[:a.runs]]))
+            X, Y, stats = X[:n_keep], Y[:n_keep], stats[:a.runs]
+        rep["data"] = {"runs": a.runs, "workers": a.workers, "pairs": int(X.shape[0]),
+                       "held_out_runs": a.val_runs, "wall_s": data_s,
                        "grid": [256, 256], "iters_per_band": a.train_iters,
                        "mean_rms_start": float(np.mean([s["rms0"] for s in stats])),
                        "mean_rms_final": float(np.mean([s["rms_final"] for s in stats]))}
