@@ -175,7 +175,7 @@ def cpu_baseline(args, sc):
     import pml_oracle as po
     import misfit_oracle as mo
     from otfwi_b200.cuda_interface_pml import pml_damping, ring_mask
-    Ts = 300
+    Ts = 1200
     dxp, dzp = pml_damping(sc.X, sc.Z, sc.PML)
     sx, sz = sc.src_xz()
     mx, mz = sc.rec_xz()
@@ -363,10 +363,13 @@ def run_ours(args):
         b.set_model(cquad=h_cq.numpy())
         b.set_observed(h_obs.numpy())
         step()  # gradient on the device (and, with several ranks, its all-reduce)
-        with torch.cuda.stream(stream):
-            h_grad.copy_(grad, non_blocking=True)
-            h_mis.copy_(mis, non_blocking=True)
         stream.synchronize()
+        # blocking copies on torch's own stream: pinned buffers used on the
+        # library's stream would be tracked by torch's host allocator, which
+        # records events on that stream when they are freed -- after the
+        # library has destroyed it
+        h_grad.copy_(grad)
+        h_mis.copy_(mis)
 
     for _ in range(max(1, args.warmup // 2)):
         e2e_step()
