@@ -968,9 +968,9 @@ int Engine::build_tables()
     utb_.ncb = NCB;
     utb_.nseg = NSEG;
     {
-        // paired kernels' counters: the ticket (first 256 bytes), then the
-        // done counts of every (shot, row segment)
-        const size_t need = 256 + sizeof(unsigned) * (size_t)std::max(cfg_.max_shots, n_shots_) * NSEG;
+        // paired kernels' counters: the tickets (one per shot, rounded up to
+        // 256 bytes), then the done counts of every (shot, row segment)
+        const size_t need = pair_ticket_bytes() + sizeof(unsigned) * (size_t)std::max(cfg_.max_shots, n_shots_) * NSEG;
         if (need > pair_sync_bytes_) {
             if (pair_sync_)
                 cudaFree(pair_sync_);
@@ -1136,17 +1136,34 @@ int Engine::launch_unfused(const StepParams &p, int kind)
 constexpr int kPairFwdMinBlocks = 24;
 constexpr int kPairRevMinBlocks = 16;
 
+// Ticket scope of the paired kernels: per shot (default) or one counter for
+// the launch (OTFWI_PAIRED_GLOBAL=1).
+static bool paired_per_shot()
+{
+    static const bool per_shot = [] {
+        const char *v = getenv("OTFWI_PAIRED_GLOBAL");
+        return !(v && v[0] == '1');
+    }();
+    return per_shot;
+}
+
 int Engine::paired_lead(int kind) const
 {
-    const int ncb = utb_.ncb, np = utb_.ncb * utb_.nseg * n_shots_;
+    const int ncb = utb_.ncb, nc = utb_.ncb * utb_.nseg;
+    const int np = paired_per_shot() ? nc : nc * n_shots_;
     int lead = pair_lead_;
     if (lead <= 0) {
-        // about one generation of resident CTAs: the awaited P items have
-        // mostly finished, their data is still in L2
-        int dev = 0, nsm = 148;
-        if (cudaGetDevice(&dev) == cudaSuccess)
-            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        lead = nsm * (kind < 2 ? kPairFwdMinBlocks : kPairRevMinBlocks);
+        if (paired_per_shot()) {
+            // half of a shot's P items ahead of its first A item
+            lead = nc / 2;
+        } else {
+            // about one generation of resident CTAs: the awaited P items
+            // have mostly finished, their data is still in L2
+            int dev = 0, nsm = 148;
+            if (cudaGetDevice(&dev) == cudaSuccess)
+                cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            lead = nsm * (kind < 2 ? kPairFwdMinBlocks : kPairRevMinBlocks);
+        }
     }
     return std::max(std::min(lead, np), std::min(2 * ncb, np));
 }
@@ -1156,18 +1173,27 @@ int Engine::launch_paired(const StepParams &p, int kind)
     PairedParams Q;
     Q.U = unfused_params(p, kind);
     Q.ticket = reinterpret_cast<unsigned long long *>(pair_sync_);
-    Q.done = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(pair_sync_) + 256);
+    Q.done = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(pair_sync_) + pair_ticket_bytes());
     Q.err = derr_;
     Q.n_shots = n_shots_;
     Q.lead = paired_lead(kind);
     Q.rec_cta = utb_.rec_cta;
     Q.rec_cta_off = utb_.rec_cta_off;
     Q.rec_cta_id = utb_.rec_cta_id;
-    const unsigned n_items = 2u * (unsigned)(Q.U.ncb * Q.U.nseg * n_shots_);
-    if (kind < 2)
-        OTF_CUDA(launch_pdl(k_paired_fwd<kPairFwdMinBlocks>, dim3(n_items), dim3(kUThreads), st_, Q));
-    else
-        OTF_CUDA(launch_pdl(k_paired_rev<kPairRevMinBlocks>, dim3(n_items), dim3(kUThreads), st_, Q));
+    const unsigned per = 2u * (unsigned)(Q.U.ncb * Q.U.nseg);
+    if (paired_per_shot()) {
+        const dim3 grid(per, (unsigned)n_shots_);
+        if (kind < 2)
+            OTF_CUDA(launch_pdl(k_paired_fwd<kPairFwdMinBlocks, true>, grid, dim3(kUThreads), st_, Q));
+        else
+            OTF_CUDA(launch_pdl(k_paired_rev<kPairRevMinBlocks, true>, grid, dim3(kUThreads), st_, Q));
+    } else {
+        const dim3 grid(per * (unsigned)n_shots_);
+        if (kind < 2)
+            OTF_CUDA(launch_pdl(k_paired_fwd<kPairFwdMinBlocks, false>, grid, dim3(kUThreads), st_, Q));
+        else
+            OTF_CUDA(launch_pdl(k_paired_rev<kPairRevMinBlocks, false>, grid, dim3(kUThreads), st_, Q));
+    }
     OTF_CUDA(cudaGetLastError());
     return 0;
 }
@@ -1178,7 +1204,7 @@ int Engine::begin_steps()
 {
     if (variant_in_use() != 5)
         return 0;
-    const size_t need = 256 + sizeof(unsigned) * (size_t)n_shots_ * utb_.nseg;
+    const size_t need = pair_ticket_bytes() + sizeof(unsigned) * (size_t)n_shots_ * utb_.nseg;
     OTF_CHECK(pair_sync_ && need <= pair_sync_bytes_, 2, "paired-kernel counters not allocated");
     OTF_CUDA(cudaMemsetAsync(pair_sync_, 0, need, st_));
     return 0;
@@ -1189,8 +1215,9 @@ int Engine::end_steps(int n_steps)
 {
     if (variant_in_use() != 5 || n_steps <= 0)
         return 0;
-    const unsigned long long per = 2ull * utb_.ncb * utb_.nseg * n_shots_;
-    k_paired_check<<<1, 1, 0, st_>>>(reinterpret_cast<const unsigned long long *>(pair_sync_),
+    const bool ps = paired_per_shot();
+    const unsigned long long per = 2ull * utb_.ncb * utb_.nseg * (ps ? 1 : n_shots_);
+    k_paired_check<<<1, 1, 0, st_>>>(reinterpret_cast<const unsigned long long *>(pair_sync_), ps ? n_shots_ : 1,
                                      per * (unsigned long long)n_steps, derr_);
     OTF_CUDA(cudaGetLastError());
     return 0;
@@ -1747,7 +1774,7 @@ extern "C" int otf_selftest_paired_faults(int *bits)
         int *err = reinterpret_cast<int *>(reinterpret_cast<char *>(buf) + 128);
         auto *ticket = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(buf) + 64);
         k_selftest_wait<<<1, 32, 0, st>>>(cnt, err);
-        otf::k_paired_check<<<1, 1, 0, st>>>(ticket, 1ull, err);
+        otf::k_paired_check<<<1, 1, 0, st>>>(ticket, 1, 1ull, err);
         if (cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess &&
             cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess) {
             *bits = h;

@@ -3,6 +3,7 @@
 // fused step kernels through captured CUDA graphs.
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <vector>
 #include "otf_common.cuh"
 #include "pml_step.cuh"
@@ -226,6 +227,10 @@ class Engine {
     void *pair_sync_ = nullptr;
     size_t pair_sync_bytes_ = 0;
     int pair_lead_ = 0;
+    size_t pair_ticket_bytes() const
+    {
+        return ((size_t)std::max(cfg_.max_shots, n_shots_) * sizeof(unsigned long long) + 255) / 256 * 256;
+    }
     int n_strips_ = 0, seg_h_ = 64;
     int *derr_ = nullptr;         // device error flag of the bounded waits
     TmaParams *tmap_ = nullptr;   // tensor maps of every field, slot and coefficient

@@ -27,6 +27,12 @@
 // the waits always end. They are bounded all the same (a timed-out wait sets
 // the device error flag; the host reports it).
 //
+// With many shots, one ticket counter is the one address every CTA of a
+// launch updates; per-shot tickets (the engine's choice) spread the updates
+// over one counter per shot: the order is then kept within each shot, which
+// is all the waits need, and the hardware's dispatch order (shot-major)
+// bounds how many shots are in flight.
+//
 // Tickets and done counts run on across the launches of one time loop (zeroed
 // by the loop's first node): launch t (t = 1 .. T-1) hands out tickets
 // [(t-1) N, t N) and a row segment is complete at t * ncb done P items. A
@@ -49,7 +55,7 @@ constexpr int kErrTicketRange = 4;    // a paired launch saw tickets outside its
 
 struct PairedParams {
     UnfusedParams U;
-    unsigned long long *ticket;  // [1] ticket counter of the time loop
+    unsigned long long *ticket;  // ticket counter of the time loop: [1], or [n_shots] with per-shot tickets
     unsigned *done;              // [n_shots][nseg] done P items per (shot, row segment)
     int *err;                    // device error flag
     int n_shots;
@@ -107,12 +113,14 @@ __device__ __forceinline__ void wait_geq(const unsigned *p, unsigned target, int
 }
 
 // Ticket of this CTA within its launch (all lanes), or ~0u after flagging a
-// ticket outside [0, n_items).
+// ticket outside [0, n_items). PER_SHOT: one counter per shot (blockIdx.y),
+// n_items of that shot.
+template <bool PER_SHOT>
 __device__ __forceinline__ unsigned paired_ticket(const PairedParams &Q, unsigned n_items)
 {
     unsigned long long k = 0;
     if (threadIdx.x == 0)
-        k = atomicAdd(Q.ticket, 1ull) - (unsigned long long)(Q.U.p.t - 1) * n_items;
+        k = atomicAdd(Q.ticket + (PER_SHOT ? blockIdx.y : 0), 1ull) - (unsigned long long)(Q.U.p.t - 1) * n_items;
     k = __shfl_sync(0xffffffffu, k, 0);
     if (k >= n_items) {
         if (threadIdx.x == 0)
@@ -143,20 +151,35 @@ __device__ __forceinline__ void paired_acquire(const PairedParams &Q, int shot, 
     __syncwarp();
 }
 
-// Forward step: grid (2 * n_shots * ncb * nseg) CTAs of one warp.
-template <int MINB>
+// The item of this CTA: global tickets order every shot's items (grid (2 *
+// n_shots * ncb * nseg)); per-shot tickets order one shot's (grid (2 * ncb *
+// nseg, n_shots)).
+template <bool PER_SHOT>
+__device__ __forceinline__ bool paired_take(const PairedParams &Q, bool &is_p, unsigned &idx)
+{
+    const unsigned nc = (unsigned)(Q.U.ncb * Q.U.nseg);
+    const unsigned np = PER_SHOT ? nc : nc * (unsigned)Q.n_shots;
+    const unsigned k = paired_ticket<PER_SHOT>(Q, 2u * np);
+    if (k == ~0u)
+        return false;
+    paired_item(k, np, (unsigned)Q.lead, is_p, idx);
+    if (PER_SHOT)
+        idx += blockIdx.y * nc;
+    return true;
+}
+
+// Forward step.
+template <int MINB, bool PER_SHOT>
 __global__ void __launch_bounds__(kUThreads, MINB) k_paired_fwd(const __grid_constant__ PairedParams Q)
 {
     pdl_enter();
     const UnfusedParams &U = Q.U;
     const StepParams &p = U.p;
-    const unsigned nc = (unsigned)(U.ncb * U.nseg), np = nc * (unsigned)Q.n_shots;
-    const unsigned k = paired_ticket(Q, 2u * np);
-    if (k == ~0u)
-        return;
+    const unsigned nc = (unsigned)(U.ncb * U.nseg);
     bool is_p;
     unsigned idx;
-    paired_item(k, np, (unsigned)Q.lead, is_p, idx);
+    if (!paired_take<PER_SHOT>(Q, is_p, idx))
+        return;
     const int shot = (int)(idx / nc), w = (int)(idx % nc), sg = w / U.ncb, cb = w % U.ncb;
     const int x = cb * kUCols + 4 * (int)threadIdx.x;
     if (is_p) {
@@ -183,19 +206,17 @@ __global__ void __launch_bounds__(kUThreads, MINB) k_paired_fwd(const __grid_con
 }
 
 // Reverse step: a P item updates both field sets of its block.
-template <int MINB>
+template <int MINB, bool PER_SHOT>
 __global__ void __launch_bounds__(kUThreads, MINB) k_paired_rev(const __grid_constant__ PairedParams Q)
 {
     pdl_enter();
     const UnfusedParams &U = Q.U;
     const StepParams &p = U.p;
-    const unsigned nc = (unsigned)(U.ncb * U.nseg), np = nc * (unsigned)Q.n_shots;
-    const unsigned k = paired_ticket(Q, 2u * np);
-    if (k == ~0u)
-        return;
+    const unsigned nc = (unsigned)(U.ncb * U.nseg);
     bool is_p;
     unsigned idx;
-    paired_item(k, np, (unsigned)Q.lead, is_p, idx);
+    if (!paired_take<PER_SHOT>(Q, is_p, idx))
+        return;
     const int shot = (int)(idx / nc), w = (int)(idx % nc), sg = w / U.ncb, cb = w % U.ncb;
     const int x = cb * kUCols + 4 * (int)threadIdx.x;
     if (is_p) {
@@ -217,12 +238,13 @@ __global__ void __launch_bounds__(kUThreads, MINB) k_paired_rev(const __grid_con
     }
 }
 
-// After a loop of paired launches: every ticket handed out exactly once, or
-// the error flag.
-__global__ void k_paired_check(const unsigned long long *ticket, unsigned long long expect, int *err)
+// After a loop of paired launches: every ticket handed out exactly once (n
+// counters), or the error flag.
+__global__ void k_paired_check(const unsigned long long *ticket, int n, unsigned long long expect, int *err)
 {
-    if (*ticket != expect)
-        atomicOr(err, kErrTicketRange);
+    for (int i = 0; i < n; i++)
+        if (ticket[i] != expect)
+            atomicOr(err, kErrTicketRange);
 }
 
 }  // namespace otf
