@@ -255,6 +255,14 @@ int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1
  * gradient dz [N][H][W][cout] of that convolution's inputs. */
 int otf_unet_conv3x3_wgrad(const void *src0, int c0, const void *src1, int c1, int up1, const void *dz,
                            int cout, float *dw, int N, int H, int W, int sm_count, void *stream);
+/* Tensor-core path of the two functions above: 1 = tcgen05 / UMMA kernels
+ * with tensor-memory accumulators (default), 0 = the warp-level mma.sync
+ * kernels; returns the previous setting (process-wide). */
+int otf_unet_set_umma(int on);
+/* Error bits of the tcgen05 kernels since the last call (1 = a bounded wait
+ * timed out: that launch's results are invalid), cleared by the call; -1 if
+ * the flag cannot be read. */
+int otf_unet_status(void);
 int otf_unet_bias_grad(const void *dz, int C, long long npix, float *db, void *stream); /* db += sum_p dz */
 int otf_unet_pool2(const void *x, void *y, int N, int H, int W, int C, void *stream);  /* 2x2 mean */
 /* dx += 0.25 * dy(parent) where x > 0 */
