@@ -128,7 +128,7 @@ int otf_batch_set_model(otf_batch *b, const float *cquad, int on_device);       
 int otf_batch_set_observed(otf_batch *b, const float *obs, int on_device);      /* [n_shots*n_rec*T] */
 int otf_batch_set_precision(otf_batch *b, int precision);
 int otf_batch_set_tile(otf_batch *b, int tile);
-/* -1 (default): automatic -- 5 with fast numerics and separable damping, 2
+/* -1 (default): automatic -- 4 with fast numerics and separable damping, 2
  * with fast numerics otherwise, 1 with faithful numerics; 0: one tile per
  * CTA per step; 1: persistent CTAs with TMA double-buffered halo tiles (tile
  * shapes 0, 1 and 4; others use 0); 2: persistent strip-split kernels, fast

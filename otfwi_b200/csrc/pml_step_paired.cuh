@@ -42,6 +42,13 @@
 //
 // Cell arithmetic is that of the unfused kernels (the same device functions):
 // results are bit-identical to them.
+//
+// Measured on one B200 (512^2, 64 shots, 300-step proxy of the gradient):
+// 0.47 ms per step at the best lead with one ticket counter, 0.58 with
+// per-shot counters, against 0.39 for the unfused kernels, which stay the
+// default. The spin on the done counts (an acquire at GPU scope per poll)
+// and the 128-register cap shared by P and A items cost more than the L2
+// re-reads save.
 #pragma once
 #include "pml_step_unfused.cuh"
 #include "tma.cuh"
