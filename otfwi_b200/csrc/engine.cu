@@ -1137,13 +1137,13 @@ int Engine::launch_unfused(const StepParams &p, int kind)
 constexpr int kPairFwdMinBlocks = 24;
 constexpr int kPairRevMinBlocks = 16;
 
-// Ticket scope of the paired kernels: per shot (default) or one counter for
-// the launch (OTFWI_PAIRED_GLOBAL=1).
+// Ticket scope of the paired kernels: one counter for the launch (default,
+// measured faster) or one per shot (OTFWI_PAIRED_PER_SHOT=1).
 static bool paired_per_shot()
 {
     static const bool per_shot = [] {
-        const char *v = getenv("OTFWI_PAIRED_GLOBAL");
-        return !(v && v[0] == '1');
+        const char *v = getenv("OTFWI_PAIRED_PER_SHOT");
+        return v && v[0] == '1';
     }();
     return per_shot;
 }

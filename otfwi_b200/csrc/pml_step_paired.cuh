@@ -28,10 +28,10 @@
 // the device error flag; the host reports it).
 //
 // With many shots, one ticket counter is the one address every CTA of a
-// launch updates; per-shot tickets (the engine's choice) spread the updates
-// over one counter per shot: the order is then kept within each shot, which
-// is all the waits need, and the hardware's dispatch order (shot-major)
-// bounds how many shots are in flight.
+// launch updates; per-shot tickets (OTFWI_PAIRED_PER_SHOT=1) spread the
+// updates over one counter per shot: the order is then kept within each
+// shot, which is all the waits need, and the hardware's dispatch order
+// (shot-major) bounds how many shots are in flight.
 //
 // Tickets and done counts run on across the launches of one time loop (zeroed
 // by the loop's first node): launch t (t = 1 .. T-1) hands out tickets
