@@ -157,7 +157,8 @@ def profile_traffic(kernel):
 def profile_value(kernel, key):
     """A 'key: N' line of the committed ncu summary of the reverse step of
     this kernel variant (None when absent)."""
-    name = {4: "reverse_step_unfused_fmc.md", 5: "reverse_step_paired_fmc.md"}.get(kernel, "reverse_step_fmc.md")
+    name = {4: "reverse_step_unfused_fmc.md", 5: "reverse_step_paired_fmc.md",
+            6: "reverse_step_fused_fmc.md"}.get(kernel, "reverse_step_fmc.md")
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
@@ -321,7 +322,10 @@ def run_ours(args):
     ach_rev = BYTES_REV * per_launch_cells / (ms_rev / 1e3) / 1e9
     ach_fwd = BYTES_FWD * per_launch_cells / (ms_fwd / 1e3) / 1e9
     tr = profile_traffic(args.kernel)
-    if args.kernel == 5:
+    if args.kernel == 6:
+        rev_name = ("k_fused_rev (reverse step in one pass: adjoint + reconstruction + imaging "
+                    "condition, all shots)")
+    elif args.kernel == 5:
         rev_name = ("k_paired_rev (reverse step in one launch: adjoint + reconstruction + imaging "
                     "condition, all shots)")
     elif args.kernel == 4:

@@ -136,8 +136,11 @@ int otf_batch_set_tile(otf_batch *b, int tile);
  * columns, fast numerics, separable damping, X a multiple of 4 (else 2); 4:
  * unfused half-steps, a launch each, fast numerics, separable damping; 5:
  * paired half-steps, both in one launch per step (P and A work items handed
- * out in order by a ticket counter), fast numerics, separable damping. 0 and
- * 1 give bit-identical results, and so do 4 and 5. */
+ * out in order by a ticket counter), fast numerics, separable damping; 6:
+ * row-lag fused half-steps, one pass over the fields per step (a warp
+ * computes P(t) of a row and the A half-step four rows behind it from a
+ * register window), fast numerics, separable damping, no ring cell listed
+ * twice (else 4). 0 and 1 give bit-identical results, and so do 4, 5 and 6. */
 int otf_batch_set_kernel(otf_batch *b, int variant);
 /* Rows per segment of the z-streaming kernels (variant 3; default 64, >= 8). */
 int otf_batch_set_stream_rows(otf_batch *b, int rows);
@@ -145,6 +148,9 @@ int otf_batch_set_stream_rows(otf_batch *b, int rows);
  * (0, the default: one generation of resident CTAs; clamped to [2 column
  * blocks, all P items]). */
 int otf_batch_set_paired_lead(otf_batch *b, int lead);
+/* Row-lag fused kernels (variant 6): rows per chunk of a CTA (default 64,
+ * >= 8; each chunk recomputes P(t) on 4 rows above and below it). */
+int otf_batch_set_fused_rows(otf_batch *b, int rows);
 /* Forward modelling of every shot; traces [n_shots][n_rec][T] (NULL: keep). */
 int otf_batch_forward(otf_batch *b, float *traces, int on_device);
 /* Forward with boundary-ring recording (gradient phase 1). */

@@ -26,7 +26,7 @@ TILES = {0: (56, 56), 1: (120, 24), 2: (120, 56), 3: (248, 24), 4: (56, 24)}
 def candidates(precision):
     c = [(1, 0), (1, 1), (1, 4), (0, 2), (0, 3)]
     if precision == 1:
-        c = [(5, 4), (4, 4), (2, 0), (2, 1), (2, 4)] + c
+        c = [(6, 4), (5, 4), (4, 4), (2, 0), (2, 1), (2, 4)] + c
     return c
 
 

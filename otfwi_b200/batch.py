@@ -40,6 +40,7 @@ def _declare(lib):
         "otf_batch_set_kernel": [c_void_p, c_int],
         "otf_batch_set_stream_rows": [c_void_p, c_int],
         "otf_batch_set_paired_lead": [c_void_p, c_int],
+        "otf_batch_set_fused_rows": [c_void_p, c_int],
         "otf_batch_forward": [c_void_p, c_void_p, c_int],
         "otf_batch_forward_ring": [c_void_p, c_void_p, c_int],
         "otf_batch_gradient": [c_void_p, c_int, c_void_p, c_void_p, c_int],
@@ -189,8 +190,13 @@ class ShotBatch:
         TMA-pipelined CTAs; 2: persistent strip-split kernels (fast numerics);
         3: z-streaming strips (fast numerics); 4: unfused streaming
         half-steps (fast numerics); 5: paired half-steps, one launch per
-        step (fast numerics)."""
+        step (fast numerics); 6: row-lag fused half-steps, one pass per step
+        (fast numerics)."""
         self._ok(self._lib.otf_batch_set_kernel(self._h, variant))
+
+    def set_fused_rows(self, rows):
+        """Rows per chunk of the row-lag fused kernels (variant 6, >= 8)."""
+        self._ok(self._lib.otf_batch_set_fused_rows(self._h, int(rows)))
 
     def set_paired_lead(self, lead):
         """P items issued before the first A item by the paired kernels

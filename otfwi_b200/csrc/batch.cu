@@ -68,6 +68,13 @@ int otf_batch_set_precision(otf_batch *b, int precision) { return b->eng.set_pre
 int otf_batch_set_tile(otf_batch *b, int tile) { return b->eng.set_tile(tile); }
 int otf_batch_set_kernel(otf_batch *b, int variant) { return b->eng.set_variant(variant); }
 int otf_batch_set_stream_rows(otf_batch *b, int rows) { return b->eng.set_stream_rows(rows); }
+int otf_batch_set_fused_rows(otf_batch *b, int rows)
+{
+    OTF_CHECK(rows >= 8, 1, "fused rows per chunk must be >= 8");
+    b->eng.set_fused_rows(rows);
+    return 0;
+}
+
 int otf_batch_set_paired_lead(otf_batch *b, int lead)
 {
     OTF_CHECK(lead >= 0, 1, "paired lead must be >= 0");

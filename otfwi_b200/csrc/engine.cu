@@ -12,6 +12,7 @@
 #include "misfit.h"
 #include "pml_step_unfused.cuh"
 #include "pml_step_paired.cuh"
+#include "pml_step_fused.cuh"
 
 namespace otf {
 
@@ -883,6 +884,81 @@ int Engine::build_tables()
             edge = x < 4 || x >= X - 4 || hdampx_[x + PAD] != 1.f;
         h.push_back(edge ? 1 : 0);
     }
+    // row-lag fused kernels: the ring index of every cell (padded layout, -1
+    // elsewhere) and per-row CSR lists of the source cells, the injectable
+    // receiver cells and every receiver
+    const size_t o_fmap = h.size();
+    fused_ok_ = true;
+    {
+        const size_t cells = (size_t)L_.rows * L_.pitch;
+        h.insert(h.end(), cells, -1);
+        for (int n = 0; n < n_ring_; n++) {
+            int &m = h[o_fmap + (size_t)L_.at(ring_x_[n], ring_z_[n])];
+            if (m >= 0)
+                fused_ok_ = false;  // a cell listed twice: one map entry cannot hold both
+            m = n;
+        }
+    }
+    auto row_cells = [&](std::vector<std::array<int, 3>> pts, size_t &o_rp, size_t &o_cx, size_t &o_ce,
+                         size_t &o_id) {
+        // pts: (z, x, id); cells in row order, ids increasing within a cell
+        std::sort(pts.begin(), pts.end());
+        std::vector<int> rp(Z + 1, 0), cx, ce(1, 0), id;
+        for (size_t e = 0; e < pts.size(); e++) {
+            if (e == 0 || pts[e][0] != pts[e - 1][0] || pts[e][1] != pts[e - 1][1]) {
+                if (e > 0)
+                    ce.push_back((int)e);
+                cx.push_back(pts[e][1]);
+                rp[pts[e][0] + 1]++;
+            }
+            id.push_back(pts[e][2]);
+        }
+        ce.push_back((int)pts.size());
+        for (int z = 0; z < Z; z++)
+            rp[z + 1] += rp[z];
+        o_rp = h.size();
+        h.insert(h.end(), rp.begin(), rp.end());
+        o_cx = h.size();
+        h.insert(h.end(), cx.begin(), cx.end());
+        h.push_back(0);
+        o_ce = h.size();
+        h.insert(h.end(), ce.begin(), ce.end());
+        o_id = h.size();
+        h.insert(h.end(), id.begin(), id.end());
+        h.push_back(0);
+    };
+    size_t f_src[4], f_rcv[4], f_rec[4];
+    {
+        std::vector<std::array<int, 3>> pts;
+        for (int k = 0; k < n_src_; k++)
+            pts.push_back({src_z_[k], src_x_[k], k});
+        row_cells(pts, f_src[0], f_src[1], f_src[2], f_src[3]);
+        pts.clear();
+        for (int n = 0; n < n_rec_; n++)
+            if (interior(rec_x_[n], rec_z_[n], X, Z))
+                pts.push_back({rec_z_[n], rec_x_[n], n});
+        row_cells(pts, f_rcv[0], f_rcv[1], f_rcv[2], f_rcv[3]);
+        // every receiver its own entry (cells may repeat): ce is unused
+        pts.clear();
+        for (int n = 0; n < n_rec_; n++)
+            pts.push_back({rec_z_[n], rec_x_[n], n});
+        std::sort(pts.begin(), pts.end());
+        std::vector<int> rp(Z + 1, 0);
+        for (auto &e : pts)
+            rp[e[0] + 1]++;
+        for (int z = 0; z < Z; z++)
+            rp[z + 1] += rp[z];
+        f_rec[0] = h.size();
+        h.insert(h.end(), rp.begin(), rp.end());
+        f_rec[1] = h.size();
+        for (auto &e : pts)
+            h.push_back(e[1]);
+        h.push_back(0);
+        f_rec[2] = h.size();
+        for (auto &e : pts)
+            h.push_back(e[2]);
+        h.push_back(0);
+    }
     if (h.size() > tabs_cap_) {
         if (tabs_)
             cudaFree(tabs_);
@@ -967,6 +1043,18 @@ int Engine::build_tables()
     utb_.rec_cta_id = utb_.rec_cta_off + n_rec_ + 1;
     utb_.ncb = NCB;
     utb_.nseg = NSEG;
+    ftb_.ringmap = d + o_fmap;
+    ftb_.src_rp = d + f_src[0];
+    ftb_.src_cx = d + f_src[1];
+    ftb_.src_ce = d + f_src[2];
+    ftb_.src_id = d + f_src[3];
+    ftb_.rcv_rp = d + f_rcv[0];
+    ftb_.rcv_cx = d + f_rcv[1];
+    ftb_.rcv_ce = d + f_rcv[2];
+    ftb_.rcv_id = d + f_rcv[3];
+    ftb_.rec_rp = d + f_rec[0];
+    ftb_.rec_cx = d + f_rec[1];
+    ftb_.rec_id = d + f_rec[2];
     {
         // paired kernels' counters: the tickets (one per shot, rounded up to
         // 256 bytes), then the done counts of every (shot, row segment)
@@ -1052,6 +1140,8 @@ int Engine::variant_in_use() const
     // half-steps in one launch, P and A items ordered by tickets) run the same
     // device functions and are selectable (measured slower: 0.47 against
     // 0.39 ms per gradient step at 512^2 x 64 shots)
+    if (variant_ == 6 && cfg_.precision == kFast && sep_ && fused_ok_)
+        return 6;
     if (variant_ == 5 && cfg_.precision == kFast && sep_)
         return 5;
     if ((variant_ == 4 || variant_ < 0) && cfg_.precision == kFast && sep_)
@@ -1199,6 +1289,39 @@ int Engine::launch_paired(const StepParams &p, int kind)
     return 0;
 }
 
+// Row-lag fused launches (pml_step_fused.cuh): one per step, no dependency
+// between CTAs; register caps from the kernels' own needs.
+constexpr int kFusedFwdMinBlocks = 16;
+constexpr int kFusedRevMinBlocks = 6;
+
+int Engine::launch_fused(const StepParams &p, int kind)
+{
+    FusedParams F;
+    F.p = p;
+    F.nxb = (cfg_.X + kFInner - 1) / kFInner;
+    F.chunk = fused_rows_;
+    F.ringmap = ftb_.ringmap;
+    F.src_rp = ftb_.src_rp;
+    F.src_cx = ftb_.src_cx;
+    F.src_ce = ftb_.src_ce;
+    F.src_id = ftb_.src_id;
+    F.rcv_rp = ftb_.rcv_rp;
+    F.rcv_cx = ftb_.rcv_cx;
+    F.rcv_ce = ftb_.rcv_ce;
+    F.rcv_id = ftb_.rcv_id;
+    F.rec_rp = ftb_.rec_rp;
+    F.rec_cx = ftb_.rec_cx;
+    F.rec_id = ftb_.rec_id;
+    F.record_ring = kind == 1;
+    const dim3 grid((unsigned)F.nxb, (unsigned)((cfg_.Z + F.chunk - 1) / F.chunk), (unsigned)n_shots_);
+    if (kind < 2)
+        OTF_CUDA(launch_pdl(k_fused_fwd<kFusedFwdMinBlocks>, grid, dim3(kFLanes), st_, F));
+    else
+        OTF_CUDA(launch_pdl(k_fused_rev<kFusedRevMinBlocks>, grid, dim3(2 * kFLanes), st_, F));
+    OTF_CUDA(cudaGetLastError());
+    return 0;
+}
+
 // Before a time loop of step launches: the paired kernels' tickets and done
 // counts start from zero.
 int Engine::begin_steps()
@@ -1264,6 +1387,8 @@ int Engine::launch_forward_step(const StepParams &p, bool with_ring, dim3 grid, 
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
     const int v = variant_in_use();
+    if (v == 6)
+        return launch_fused(p, with_ring ? 1 : 0);
     if (v == 5)
         return launch_paired(p, with_ring ? 1 : 0);
     if (v == 4)
@@ -1301,6 +1426,8 @@ int Engine::launch_reverse_step(const StepParams &p, dim3 grid, int pin, int ain
 {
     const KernelSet &k = ktable().s[cfg_.tile][cfg_.precision][sep_ ? 1 : 0];
     const int v = variant_in_use();
+    if (v == 6)
+        return launch_fused(p, 2);
     if (v == 5)
         return launch_paired(p, 2);
     if (v == 4)
@@ -1370,7 +1497,7 @@ int Engine::set_stream_rows(int rows)
 
 int Engine::set_variant(int variant)
 {
-    OTF_CHECK(variant >= -1 && variant <= 5, 1, "unknown kernel variant");
+    OTF_CHECK(variant >= -1 && variant <= 6, 1, "unknown kernel variant");
     if (variant != variant_) {
         variant_ = variant;
         drop_graphs();

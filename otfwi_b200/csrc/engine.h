@@ -111,12 +111,16 @@ class Engine {
     // 2 persistent strip-split (fast numerics); 3 z-streaming strips (fast
     // numerics, separable damping, X a multiple of 4); 4 unfused streaming
     // half-steps (fast numerics, separable damping); 5 paired half-steps, one
-    // launch per step (fast numerics, separable damping). Falls back where
-    // not compiled or not applicable.
+    // launch per step (fast numerics, separable damping); 6 row-lag fused
+    // half-steps, one pass per step (fast numerics, separable damping, no
+    // ring cell listed twice). Falls back where not compiled or not
+    // applicable.
     int set_variant(int variant);
     // paired kernels: P items issued before the first A item (0 = one
     // generation of resident CTAs)
     void set_paired_lead(int lead) { pair_lead_ = lead; drop_graphs(); }
+    // fused kernels: rows per chunk (>= 8)
+    void set_fused_rows(int rows) { fused_rows_ = rows < 8 ? 8 : rows; drop_graphs(); }
     // rows per segment of the z-streaming kernels (>= 8)
     int set_stream_rows(int rows);
     int variant_in_use() const;
@@ -140,6 +144,7 @@ class Engine {
     int launch_stream(const StepParams &p, int kind);  // 0 forward, 1 forward + ring, 2 reverse
     int launch_unfused(const StepParams &p, int kind);  // 0 forward, 1 forward + ring, 2 reverse
     int launch_paired(const StepParams &p, int kind);   // 0 forward, 1 forward + ring, 2 reverse
+    int launch_fused(const StepParams &p, int kind);    // 0 forward, 1 forward + ring, 2 reverse
     UnfusedParams unfused_params(const StepParams &p, int kind) const;
     int paired_lead(int kind) const;
     int begin_steps();             // before a time loop of step launches
@@ -222,6 +227,13 @@ class Engine {
         const int *rec_cta, *rec_cta_off, *rec_cta_id;  // every receiver grouped by owning block
         int n_src_cells, n_rcv_cells, ncb, nseg;
     } utb_{};
+    // row-lag fused kernels: ring index map and per-row point lists (in tabs_)
+    struct {
+        const int *ringmap, *src_rp, *src_cx, *src_ce, *src_id, *rcv_rp, *rcv_cx, *rcv_ce, *rcv_id;
+        const int *rec_rp, *rec_cx, *rec_id;
+    } ftb_{};
+    bool fused_ok_ = true;   // no ring cell listed twice
+    int fused_rows_ = 64;    // rows per chunk of the fused kernels
     // paired kernels: ticket counter (first 256 bytes) and done counts
     // [max_shots][nseg]
     void *pair_sync_ = nullptr;
