@@ -886,7 +886,11 @@ int Engine::build_tables()
     }
     // row-lag fused kernels: the ring index of every cell (padded layout, -1
     // elsewhere) and per-row CSR lists of the source cells, the injectable
-    // receiver cells and every receiver
+    // receiver cells and every receiver. The map is read 4 cells (16 bytes)
+    // at a time, so it starts on a 16-byte boundary of the table (cudaMalloc
+    // aligns the table itself to 256 bytes).
+    while (h.size() % 4)
+        h.push_back(0);
     const size_t o_fmap = h.size();
     fused_ok_ = true;
     {
@@ -1213,8 +1217,7 @@ int Engine::launch_unfused(const StepParams &p, int kind)
         const int tail = (extra + per_row - 1) / per_row;
         OTF_CUDA(launch_pdl(k_unfused_a_fwd, dim3(U.ncb, U.nseg + tail, n_shots_), dim3(kUThreads), st_, U));
     } else {
-        OTF_CUDA(launch_pdl(k_unfused_p_rev, dim3(U.ncb, U.nseg, 2 * n_shots_), dim3(kUThreads), st_, U,
-                            n_shots_));
+        OTF_CUDA(launch_pdl(k_unfused_p_rev, dim3(U.ncb, U.nseg, 2 * n_shots_), dim3(kUThreads), st_, U));
         OTF_CUDA(launch_pdl(k_unfused_a_rev, grid, dim3(kUThreads), st_, U));
     }
     OTF_CUDA(cudaGetLastError());

@@ -27,6 +27,15 @@
 // reverse step, against 28 and 64 for the fused kernels, at 80-90% of the
 // bandwidth instead of under 50%.
 //
+// Shot order alternates between consecutive launches: CTAs are dispatched in
+// grid order, the P kernels walk the shots upwards and the A kernels
+// downwards, so each launch begins on the shots its predecessor finished
+// with, whose fields may still be in the L2 (P(t) and Ax, Az (t-1) for the A
+// kernel; P(t) and Ax, Az (t) for the next P kernel). The order of CTAs
+// changes no result: every cell and every shot's gradient is written by one
+// thread. Measured on one B200 (64 shots, 512^2): forward step 0.119 ms
+// against 0.123 in launch order, reverse step unchanged (0.27 ms).
+//
 // The cell arithmetic is that of the strip-split kernels: the same pair-form
 // staggered sums, P and Q updates, injection (after the cell's update, in
 // source order) and Laplacian; the damped
@@ -224,7 +233,8 @@ __device__ __forceinline__ void cta_inject(const StepParams &p, const Fields &f,
 constexpr int kUPMinBlocks = 24;
 constexpr int kUAMinBlocks = 28;
 
-// Forward P half-step and the sources: grid (ncb, nseg, n_shots).
+// Forward P half-step and the sources: grid (ncb, nseg, n_shots), shots
+// upwards.
 __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
@@ -236,17 +246,17 @@ __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const
     cta_inject(U.p, U.p.f0, blockIdx.z, U.src_cta, U.src_off, U.src_ptr, U.src_id, cta, true);
 }
 
-// Reverse P half-steps of both sets: grid (ncb, nseg, 2 * n_shots); z <
-// n_shots: reconstruction (set 0, q0) then the ring overwrite, else adjoint
-// (set 1, q1) then the adjoint sources.
-__global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_rev(const __grid_constant__ UnfusedParams U, int n_shots)
+// Reverse P half-steps of both sets: grid (ncb, nseg, 2 * n_shots), shot
+// z / 2 upwards; even z: reconstruction (set 0, q0) then the ring
+// overwrite, odd z: adjoint (set 1, q1) then the adjoint sources.
+__global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_rev(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
     const StepParams &p = U.p;
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     const int cta = blockIdx.x + U.ncb * blockIdx.y;
-    const bool rec_set = (int)blockIdx.z < n_shots;
-    const int shot = rec_set ? (int)blockIdx.z : (int)blockIdx.z - n_shots;
+    const bool rec_set = (blockIdx.z & 1u) == 0u;
+    const int shot = (int)(blockIdx.z >> 1);
     if (x < p.X) {
         if (rec_set)
             p_segment<true>(U, p.f0, p.q0, shot, x, blockIdx.y * kURows);
@@ -347,14 +357,15 @@ __device__ __forceinline__ void a_fwd_segment(const UnfusedParams &U, int shot, 
     }
 }
 
-// Forward A half-step: grid (ncb, n_tail + nseg, n_shots); the first n_tail
-// rows of CTAs record the receivers (and the ring) of their shot: first, so
-// that these latency-bound CTAs run beside the stencil CTAs, not after them.
+// Forward A half-step: grid (ncb, n_tail + nseg, n_shots), shots downwards;
+// the first n_tail rows of CTAs record the receivers (and the ring) of their
+// shot: first, so that these latency-bound CTAs run beside the stencil CTAs,
+// not after them.
 __global__ void __launch_bounds__(kUThreads, kUAMinBlocks) k_unfused_a_fwd(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
     const StepParams &p = U.p;
-    const int shot = blockIdx.z;
+    const int shot = (int)(gridDim.z - 1u - blockIdx.z);
     const int64_t so = p.shot_stride * shot;
     const float *__restrict__ P = p.f0.px_out + so;
     const int n_tail = gridDim.y - U.nseg;
@@ -486,14 +497,14 @@ __device__ __forceinline__ void a_rev_segment(const UnfusedParams &U, int shot, 
 }
 
 // Reverse A half-steps of both sets and the imaging condition: grid (ncb,
-// nseg, n_shots).
+// nseg, n_shots), shots downwards.
 __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= U.p.X)
         return;
-    a_rev_segment<false>(U, blockIdx.z, x, blockIdx.y * kURows);
+    a_rev_segment<false>(U, (int)(gridDim.z - 1u - blockIdx.z), x, blockIdx.y * kURows);
 }
 
 }  // namespace otf
