@@ -262,8 +262,10 @@ int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1
 int otf_unet_conv3x3_wgrad(const void *src0, int c0, const void *src1, int c1, int up1, const void *dz,
                            int cout, float *dw, int N, int H, int W, int sm_count, void *stream);
 /* Tensor-core path of the two functions above: 1 = tcgen05 / UMMA kernels
- * with tensor-memory accumulators (default), 0 = the warp-level mma.sync
- * kernels; returns the previous setting (process-wide). */
+ * with tensor-memory accumulators (default; the weight gradient of layers
+ * with cin x cout below 128 x 128 keeps the mma.sync kernel, measured faster
+ * there), 2 = tcgen05 for every shape, 0 = the warp-level mma.sync kernels;
+ * returns the previous setting (process-wide). */
 int otf_unet_set_umma(int on);
 /* Error bits of the tcgen05 kernels since the last call (1 = a bounded wait
  * timed out: that launch's results are invalid), cleared by the call; -1 if

@@ -21,6 +21,9 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <cstring>
+#include <string>
+#include <cudaTypedefs.h>
 #include "otf_common.cuh"
 #include "tma.cuh"
 
@@ -561,6 +564,64 @@ using namespace otf::unet;
 namespace {
 int g_use_umma = 1;
 bool use_umma() { return g_use_umma != 0; }
+
+// Tiled BF16 tensor map (rank 3 or 4, no swizzle, zero fill outside).
+int encode_bf16_map(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
+                    const cuuint32_t *box)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        OTF_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        OTF_CHECK(q == cudaDriverEntryPointSuccess && p, 4, "cuTensorMapEncodeTiled is unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void *>(base), dims,
+                          strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    OTF_CHECK(r == CUDA_SUCCESS, 4, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+    return 0;
+}
+
+// The maps of k_conv3x3_umma: weights (cin, cout, 9) with box (8, nb, 9);
+// the inputs (c, W, H, N) with box (8, 10, 34, 1).
+int conv_maps(ConvMaps *m, const ConvArgs &a, int nb)
+{
+    std::memset(m, 0, sizeof(*m));
+    const int cin = a.c0 + a.c1;
+    {
+        const cuuint64_t dims[3] = {(cuuint64_t)cin, (cuuint64_t)a.cout, 9};
+        const cuuint64_t str[2] = {(cuuint64_t)cin * 2, (cuuint64_t)a.cout * cin * 2};
+        const cuuint32_t box[3] = {8, (cuuint32_t)nb, 9};
+        if (encode_bf16_map(&m->w, a.w, 3, dims, str, box))
+            return -1;
+    }
+    const cuuint32_t box[4] = {8, (cuuint32_t)umma::HWU, (cuuint32_t)umma::HH2, 1};
+    for (int i = 0; i < 2; i++) {
+        const int c = i ? a.c1 : a.c0;
+        if (c == 0 || (i == 1 && a.up1))
+            continue;
+        const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.N};
+        const cuuint64_t str[3] = {(cuuint64_t)c * 2, (cuuint64_t)a.W * c * 2, (cuuint64_t)a.H * a.W * c * 2};
+        if (encode_bf16_map(i ? &m->x1 : &m->x0, i ? (const void *)a.src1 : (const void *)a.src0, 4, dims, str, box))
+            return -1;
+    }
+    return 0;
+}
+
+// Stages of k_conv3x3_umma for nb output channels: as many as fit two CTAs
+// per SM (one CTA for 256 channels), at most 4.
+int conv_stages(int nb)
+{
+    if (nb > 128)
+        return 2;
+    int nst = 4;
+    while (nst > 2 && umma_smem_bytes(nb, nst) > 113 * 1024)
+        nst--;
+    return nst;
+}
 inline unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 int launch_status()
 {
@@ -610,17 +671,16 @@ int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1
         for (int c : {256, 128, 64, 32})
             if (nb > 256 && cout % c == 0)
                 nb = c;
-        const int tiles = ((W + umma::TWU - 1) / umma::TWU) * ((H + umma::THU - 1) / umma::THU) * N;
+        const int tiles = ((W + umma::TWU - 1) / umma::TWU) * ((H + umma::TH2 - 1) / umma::TH2) * N;
         const dim3 grid((unsigned)tiles, (unsigned)(cout / nb));
-        if (nb > 128) {
-            const int smem = umma_smem_bytes(nb, 2);
-            OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_umma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            k_conv3x3_umma<2><<<grid, 128, smem, (cudaStream_t)stream>>>(a, nb);
-        } else {
-            const int smem = umma_smem_bytes(nb, 3);
-            OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_umma<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            k_conv3x3_umma<3><<<grid, 128, smem, (cudaStream_t)stream>>>(a, nb);
-        }
+        ConvMaps maps;
+        if (conv_maps(&maps, a, nb))
+            return -1;
+        const int nst = conv_stages(nb);
+        const int smem = umma_smem_bytes(nb, nst);
+        auto kern = nst == 2 ? k_conv3x3_umma<2> : nst == 3 ? k_conv3x3_umma<3> : k_conv3x3_umma<4>;
+        OTF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        kern<<<grid, 128, smem, (cudaStream_t)stream>>>(a, maps, nb);
         return launch_status();
     }
     const int tiles = ((W + TW - 1) / TW) * ((H + TH - 1) / TH) * N;
@@ -629,12 +689,14 @@ int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1
 }
 
 /* Tensor-core path of the 3x3 convolution and its weight gradient: 1 =
- * tcgen05 (default), 0 = the warp-level mma.sync kernels; returns the
- * previous setting. */
+ * tcgen05 (default; the weight gradient of layers with cin x cout below
+ * 128 x 128 keeps the mma.sync kernel, which is faster there), 2 = tcgen05
+ * for every shape, 0 = the warp-level mma.sync kernels; returns the previous
+ * setting. */
 int otf_unet_set_umma(int on)
 {
     const int prev = g_use_umma;
-    g_use_umma = on ? 1 : 0;
+    g_use_umma = on < 0 ? 0 : (on > 2 ? 2 : on);
     return prev;
 }
 
@@ -670,7 +732,11 @@ int otf_unet_conv3x3_wgrad(const void *src0, int c0, const void *src1, int c1, i
     a.N = N;
     a.H = H;
     a.W = W;
-    if (use_umma()) {
+    // The tcgen05 weight gradient computes 128 output channels per CTA (rows
+    // beyond cout are zeros): measured per layer of the 16 x 256^2 network it
+    // beats the mma.sync kernel where cin x cout >= 128 x 128 (1.1-1.8x) and
+    // loses below (0.6-0.9x), so smaller layers keep the mma.sync kernel.
+    if (use_umma() && (g_use_umma == 2 || (int64_t)(c0 + c1) * cout >= 128 * 128)) {
         // tensor-core path: 128 output channels x 32 (or 16) input channels x
         // 9 taps per CTA, the pixels split into slab ranges so that about one
         // CTA per SM (two with 16 input channels) runs

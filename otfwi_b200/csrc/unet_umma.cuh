@@ -1,31 +1,39 @@
 // 3x3 convolution on the 5th-generation tensor cores (tcgen05 / UMMA) for
-// the preconditioner U-Net: an implicit GEMM with
+// the preconditioner U-Net: an implicit GEMM per CTA with
 //
-//   M = 128 output pixels (a tile 8 wide x 16 tall of one image),
-//   N = every output channel of the CTA (cout, or 256 of them, <= 256),
+//   M = 256 output pixels (a tile 8 wide x 32 tall of one image), as two
+//       128-row MMAs (tile rows 0-15 and 16-31) that share every weight stage,
+//   N = the CTA's output channels (cout, or a block of 256, <= 256),
 //   K = 9 taps x the input channels, taken 16 channels (one MMA K) at a time.
 //
-// Per 16-channel chunk the CTA stages, with cp.async (zero fill at the image
-// border; the second input upsampled on load as in k_conv3x3), the input halo
-// (18 x 10 pixels) as two 8-channel planes [pixel][8 channels], and the
-// chunk's weights of every tap as [tap][plane][cout][8 channels]. Both are
-// the no-swizzle K-major canonical UMMA layout: a core matrix is 8 rows of 16
-// bytes. For tap (dy, dx) the A operand is the halo shifted by (dy, dx):
-// row m of A (output pixel oy = m / 8, ox = m % 8) is halo pixel (oy + dy) *
-// 10 + ox + dx, so 8 consecutive rows are 8 consecutive halo pixels (one core
-// matrix), consecutive core matrices are one halo row (160 bytes) apart, and
-// the second K half is the other plane: one descriptor per tap, no copy. One
-// thread issues the 9 MMAs of a chunk (tcgen05.mma kind::f16, BF16 inputs,
-// FP32 accumulators in tensor memory, 128 lanes x N columns) and commits
-// them to the stage's mbarrier; the stage is refilled once that barrier
-// completes. The epilogue reads the accumulators with tcgen05.ld (warp w owns
-// lanes 32w .. 32w+31, i.e. tile rows 4w .. 4w+3), adds the bias, applies the
-// ReLU and the optional masks, and writes BF16 to the split outputs as
-// k_conv3x3 does.
+// Warp roles, each stage a full / empty mbarrier pair:
+//   warp 0 (producer): per 16-channel chunk, the chunk's weights of every tap
+//     ([tap][cout][8 ch] per 8-channel plane: one 3D TMA load per plane) and
+//     the input halo (34 x 10 pixels x 8 channels per plane: one 4D TMA load
+//     per plane; the tensor map's zero fill supplies the image border); a
+//     chunk of the upsampled second input is gathered by the warp with
+//     cp.async instead (nearest upsampling on load), then made visible to the
+//     tensor cores (fence.proxy.async) before the stage's arrival;
+//   warp 1 (one thread): waits for a stage, issues its 18 MMAs (9 taps x 2
+//     halves; kind::f16, BF16 in, FP32 accumulators in tensor memory, 2 x N
+//     columns), and commits them to the stage's empty barrier;
+//   then all four warps: the epilogue reads the accumulators with tcgen05.ld
+//     (warp w owns TMEM lanes 32w .. 32w+31), adds the bias, applies the ReLU
+//     and the optional masks, and writes BF16 (16-byte stores) to the split
+//     outputs as k_conv3x3 does.
+// Both operands use the no-swizzle K-major canonical layout: a core matrix is
+// 8 rows of 16 bytes. For tap (dy, dx) and half h the A operand starts at halo
+// pixel (dy + 16 h) * 10 + dx: row m (pixel oy = m / 8, ox = m % 8) is 8
+// consecutive halo pixels per core matrix, core matrices one halo row (160
+// bytes) apart, the second K half in the other plane -- one descriptor per
+// (tap, half), no copy.
+//
+// The weight gradient (k_conv3x3_wgrad_umma, below) keeps the 128-pixel slab
+// (8 x 16) of the first version.
 //
 // Every mbarrier wait is bounded (tma.cuh: 0.5 s); on expiry the kernel sets
-// the error flag, skips its remaining MMAs and epilogue, waits (bounded) for
-// the MMAs it issued, frees its tensor memory and exits.
+// the error flag, stops issuing, waits (bounded) for the copies and MMAs it
+// issued, skips the epilogue, frees its tensor memory and exits.
 #pragma once
 // included inside namespace otf::unet by unet.cu, after tma.cuh
 
@@ -111,35 +119,54 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v)
 
 }  // namespace umma
 
-// dynamic shared memory of the UMMA conv: NST stages of (halo + weights),
-// the stage barriers and the tensor-memory address slot
-__host__ __device__ constexpr int umma_stage_bytes(int n) { return umma::A_BYTES + 9 * 2 * n * 16; }
-__host__ __device__ constexpr int umma_smem_bytes(int n, int nst) { return nst * umma_stage_bytes(n) + 128; }
-
 __device__ int g_unet_err;  // set by a timed-out wait of a U-Net tensor-core kernel
 
-// One CTA: 128 output pixels (8 x 16) of one image x N output channels
-// (blockIdx.y selects the block of N channels); 4 warps.
+namespace umma {
+constexpr int TH2 = 32;                                    // output tile height: 8 x 32 = 256 pixels
+constexpr int HH2 = TH2 + 2;                               // halo 10 x 34
+constexpr int HPIX2 = HWU * HH2;                           // 340 halo pixels
+constexpr int PLANE2 = ((HPIX2 * 16 + 127) / 128) * 128;   // one 8-channel halo plane, 128-byte aligned
+}  // namespace umma
+
+// Tensor maps of one convolution: weights [9][cout][cin] as (cin, cout, 9),
+// box (8, N, 9); the inputs [N][H][W][c] as (c, W, H, N), box (8, 10, 34, 1)
+// (x1: the second input at full resolution; unused when it is upsampled).
+struct ConvMaps {
+    CUtensorMap w, x0, x1;
+};
+
+// dynamic shared memory: NST stages of (two halo planes, two weight planes),
+// then 2 NST + 1 barriers, the tensor-memory slot and the failure flag
+__host__ __device__ constexpr int umma_stage_bytes(int n) { return 2 * umma::PLANE2 + 2 * 9 * n * 16; }
+__host__ __device__ constexpr int umma_smem_bytes(int n, int nst) { return nst * umma_stage_bytes(n) + 256; }
+
 template <int NST>
-__global__ void __launch_bounds__(128) k_conv3x3_umma(ConvArgs a, int N)
+__global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ ConvArgs a,
+                                                      const __grid_constant__ ConvMaps maps, int N)
 {
-    extern __shared__ __align__(128) unsigned char smu[];
+    extern __shared__ __align__(1024) unsigned char smu[];
     const int sb = umma_stage_bytes(N);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smu + NST * sb);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + NST + 1);
-    const int tiles_x = (a.W + umma::TWU - 1) / umma::TWU, tiles_y = (a.H + umma::THU - 1) / umma::THU;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smu + NST * sb);
+    uint64_t *empty = full + NST;
+    uint64_t *done = empty + NST;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
+    int *fail = reinterpret_cast<int *>(tslot + 1);
+    const int tiles_x = (a.W + umma::TWU - 1) / umma::TWU, tiles_y = (a.H + umma::TH2 - 1) / umma::TH2;
     int bidx = blockIdx.x;
     const int n = bidx / (tiles_x * tiles_y);
     bidx -= n * tiles_x * tiles_y;
     const int ty = bidx / tiles_x, tx = bidx - ty * tiles_x;
-    const int y0 = ty * umma::THU, x0 = tx * umma::TWU, co0 = blockIdx.y * N;
+    const int y0 = ty * umma::TH2, x0 = tx * umma::TWU, co0 = blockIdx.y * N;
     const int cin = a.c0 + a.c1, nk = cin / KC;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t ncols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
+    uint32_t ncols = 32;
+    while (ncols < 2u * (uint32_t)N)
+        ncols <<= 1;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s <= NST; s++)
-            otf::mbar_init(&bar[s], 1);
+        for (int s = 0; s < 2 * NST + 1; s++)
+            otf::mbar_init(&full[s], 1);
+        *fail = 0;
         otf::fence_barrier_init();
     }
     if (warp == 0)
@@ -148,100 +175,169 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(ConvArgs a, int N)
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t idesc = umma::instr_desc_bf16(N);
 
-    auto load = [&](int kc, unsigned char *st) {
-        uint32_t *sa = reinterpret_cast<uint32_t *>(st);
-        for (int i = threadIdx.x; i < umma::HPIX * 2; i += 128) {
-            const int px = i >> 1, half = i & 1;
-            const int hy = px / umma::HWU, hx = px - hy * umma::HWU;
-            const int gy = y0 + hy - 1, gx = x0 + hx - 1;
-            const bool ok = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
-            const void *src = ok ? (const void *)in_ptr(a, n, gy, gx, kc * KC + half * 8) : (const void *)a.w;
-            cp_async16(sa + (half * umma::PLANE_A + px * 16) / 4, src, ok ? 16 : 0);
+    if (warp == 0) {
+        // producer
+        if (lane == 0) {
+            otf::tma_prefetch_desc(&maps.w);
+            otf::tma_prefetch_desc(&maps.x0);
+            if (a.c1 && !a.up1)
+                otf::tma_prefetch_desc(&maps.x1);
         }
-        uint32_t *sw = reinterpret_cast<uint32_t *>(st + umma::A_BYTES);
-        for (int i = threadIdx.x; i < 9 * N * 2; i += 128) {
-            const int row = i >> 1, half = i & 1;
-            const int tap = row / N, co = row - tap * N;
-            cp_async16(sw + ((tap * 2 + half) * N + co) * 4,
-                       a.w + (int64_t)(tap * a.cout + co0 + co) * cin + kc * KC + half * 8, 16);
-        }
-    };
-
-    bool ok = true;
-    load(0, smu);
-    cp_commit();
-    for (int kc = 0; kc < nk; kc++) {
-        const int s = kc % NST;
-        if (kc + 1 < nk) {
-            const int s1 = (kc + 1) % NST;
-            // the stage's previous chunk (kc + 1 - NST) must have been consumed
-            if (kc + 1 >= NST && ok)
-                ok = otf::mbar_wait(&bar[s1], (uint32_t)(((kc + 1) / NST - 1) & 1), &g_unet_err);
-            load(kc + 1, smu + s1 * sb);
-        }
-        cp_commit();
-        cp_wait<1>();
-        umma::fence_proxy_async();  // cp.async writes -> visible to the tensor cores
-        __syncthreads();
-        if (threadIdx.x == 0 && ok) {
-            umma::fence_after_sync();
-            const uint32_t abase = otf::smem_u32(smu + s * sb);
-            const uint32_t bbase = abase + umma::A_BYTES;
-#pragma unroll
-            for (int tap = 0; tap < 9; tap++) {
-                const int dy = tap / 3, dx = tap - 3 * (tap / 3);
-                const uint64_t ad = umma::smem_desc(abase + (dy * umma::HWU + dx) * 16, umma::PLANE_A,
-                                                    umma::HWU * 16);
-                const uint64_t bd = umma::smem_desc(bbase + tap * 2 * N * 16, N * 16, 128);
-                umma::mma_bf16(tmem, ad, bd, idesc, kc > 0 || tap > 0);
+        const uint32_t wbytes = 2u * 9u * (uint32_t)N * 16u, abytes = 2u * umma::HPIX2 * 16u;
+        int issued = 0;
+        for (int kc = 0; kc < nk; kc++) {
+            const int s = kc % NST;
+            if (kc >= NST) {
+                int okw = 1;
+                if (lane == 0)
+                    okw = otf::mbar_wait(&empty[s], (uint32_t)((kc / NST - 1) & 1), &g_unet_err) ? 1 : 0;
+                if (!__shfl_sync(0xffffffffu, okw, 0)) {
+                    if (lane == 0)
+                        *fail = 1;
+                    break;
+                }
             }
-            umma::mma_commit(&bar[s]);
+            unsigned char *st = smu + s * sb;
+            const int ch = kc * KC;
+            const bool from1 = ch >= a.c0;
+            const bool gather = from1 && a.up1;
+            if (lane == 0) {
+                otf::mbar_expect_tx(&full[s], wbytes + (gather ? 0u : abytes));
+                for (int h = 0; h < 2; h++)
+                    otf::tma_load_3d(st + 2 * umma::PLANE2 + h * 9 * N * 16, &maps.w, ch + 8 * h, co0, 0, &full[s]);
+                if (!gather) {
+                    const CUtensorMap *mx = from1 ? &maps.x1 : &maps.x0;
+                    const int c = from1 ? ch - a.c0 : ch;
+                    for (int h = 0; h < 2; h++)
+                        otf::tma_load_4d(st + h * umma::PLANE2, mx, c + 8 * h, x0 - 1, y0 - 1, n, &full[s]);
+                }
+            }
+            if (gather) {
+                for (int i = lane; i < umma::HPIX2 * 2; i += 32) {
+                    const int px = i >> 1, h = i & 1;
+                    const int hy = px / umma::HWU, hx = px - hy * umma::HWU;
+                    const int gy = y0 + hy - 1, gx = x0 + hx - 1;
+                    const bool in = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
+                    const void *src = in ? (const void *)in_ptr(a, n, gy, gx, ch + 8 * h) : (const void *)a.w;
+                    cp_async16(reinterpret_cast<uint32_t *>(st + h * umma::PLANE2 + px * 16), src, in ? 16 : 0);
+                }
+                cp_commit();
+                cp_wait<0>();
+                umma::fence_proxy_async();  // cp.async writes -> visible to the tensor cores
+            }
+            __syncwarp();
+            if (lane == 0)
+                otf::mbar_arrive(&full[s]);
+            issued = kc + 1;
         }
-        __syncthreads();
+        // wait for every copy this warp issued (the last fill of each stage)
+        if (lane == 0)
+            for (int kc = issued > NST ? issued - NST : 0; kc < issued; kc++)
+                otf::mbar_wait(&full[kc % NST], (uint32_t)((kc / NST) & 1), &g_unet_err);
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = umma::instr_desc_bf16(N);
+            for (int kc = 0; kc < nk; kc++) {
+                const int s = kc % NST;
+                if (!otf::mbar_wait(&full[s], (uint32_t)((kc / NST) & 1), &g_unet_err)) {
+                    *fail = 1;
+                    break;
+                }
+                umma::fence_after_sync();
+                const uint32_t abase = otf::smem_u32(smu + s * sb);
+                const uint32_t bbase = abase + 2 * umma::PLANE2;
+#pragma unroll
+                for (int tap = 0; tap < 9; tap++) {
+                    const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+                    const uint64_t bd = umma::smem_desc(bbase + tap * N * 16, 9 * N * 16, 128);
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const uint64_t ad = umma::smem_desc(abase + ((dy + 16 * h) * umma::HWU + dx) * 16,
+                                                            umma::PLANE2, umma::HWU * 16);
+                        umma::mma_bf16(tmem + (uint32_t)(h * N), ad, bd, idesc, kc > 0 || tap > 0);
+                    }
+                }
+                umma::mma_commit(&empty[s]);
+            }
+            umma::mma_commit(done);  // arrives once every MMA issued before it has completed
+        }
+        __syncwarp();
     }
-    // all MMAs complete: one more commit (tracks every MMA issued before it)
-    if (threadIdx.x == 0)
-        umma::mma_commit(&bar[NST]);
-    const bool done = otf::mbar_wait(&bar[NST], 0, &g_unet_err);
-    ok = ok && done;
+    // every role done issuing; the accumulators are final once `done` completes
+    __syncthreads();
+    const bool ok = otf::mbar_wait(done, 0, &g_unet_err) && *fail == 0;
     umma::fence_after_sync();
 
     if (ok) {
         const int m = warp * 32 + lane;
-        const int y = y0 + m / umma::TWU, x = x0 + (m % umma::TWU);
-        const bool inside = y < a.H && x < a.W;
-        const int64_t pix = ((int64_t)n * a.H + y) * a.W + x;
-        for (int c0 = 0; c0 < N; c0 += 32) {
-            float v[32];
-            umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (!inside)
-                continue;
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+            const int y = y0 + 16 * h + m / umma::TWU, x = x0 + (m % umma::TWU);
+            const bool inside = y < a.H && x < a.W;
+            const int64_t pix = ((int64_t)n * a.H + y) * a.W + x;
+#pragma unroll 1
+            for (int c0 = 0; c0 < N; c0 += 32) {
+                float v[32];
+                umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * N + c0), v);
+                if (!inside)
+                    continue;
 #pragma unroll
-            for (int j = 0; j < 32; j += 2) {
-                const int co = co0 + c0 + j;
-                float v0 = v[j], v1 = v[j + 1];
-                if (a.bias) {
-                    v0 += a.bias[co];
-                    v1 += a.bias[co + 1];
+                for (int g = 0; g < 32; g += 8) {
+                    const int co = co0 + c0 + g;
+                    float r[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        r[j] = v[g + j];
+                        if (a.bias)
+                            r[j] += a.bias[co + j];
+                        if (a.relu)
+                            r[j] = fmaxf(r[j], 0.f);
+                    }
+                    const bool lo = co < a.split;
+                    const int cc = lo ? a.split : a.cout - a.split, ci = lo ? co : co - a.split;
+                    if (lo == (co + 7 < a.split) && ((cc | ci) & 7) == 0) {
+                        // the 8 channels on one side, 16-byte aligned
+                        bf16 *dst = (lo ? a.dst0 : a.dst1) + pix * cc + ci;
+                        const bf16 *mask = lo ? a.mask0 : a.mask1;
+                        if (mask) {
+                            const uint4 mk = *reinterpret_cast<const uint4 *>(mask + pix * cc + ci);
+                            const bf162 *m2 = reinterpret_cast<const bf162 *>(&mk);
+#pragma unroll
+                            for (int j = 0; j < 4; j++) {
+                                if (!(__low2float(m2[j]) > 0.f))
+                                    r[2 * j] = 0.f;
+                                if (!(__high2float(m2[j]) > 0.f))
+                                    r[2 * j + 1] = 0.f;
+                            }
+                        }
+                        uint4 pk;
+                        bf162 *p2 = reinterpret_cast<bf162 *>(&pk);
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            p2[j] = __floats2bfloat162_rn(r[2 * j], r[2 * j + 1]);
+                        *reinterpret_cast<uint4 *>(dst) = pk;
+                        continue;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; j += 2) {
+                        const int cj = co + j;
+                        float v0 = r[j], v1 = r[j + 1];
+                        const bool l2 = cj < a.split;
+                        bf16 *dst = l2 ? a.dst0 : a.dst1;
+                        const bf16 *mask = l2 ? a.mask0 : a.mask1;
+                        const int c2 = l2 ? a.split : a.cout - a.split, i2 = l2 ? cj : cj - a.split;
+                        if (mask) {
+                            const bf162 mk = *reinterpret_cast<const bf162 *>(mask + pix * c2 + i2);
+                            if (!(__low2float(mk) > 0.f))
+                                v0 = 0.f;
+                            if (!(__high2float(mk) > 0.f))
+                                v1 = 0.f;
+                        }
+                        *reinterpret_cast<bf162 *>(dst + pix * c2 + i2) = __floats2bfloat162_rn(v0, v1);
+                    }
                 }
-                if (a.relu) {
-                    v0 = fmaxf(v0, 0.f);
-                    v1 = fmaxf(v1, 0.f);
-                }
-                const bool lo = co < a.split;
-                bf16 *dst = lo ? a.dst0 : a.dst1;
-                const bf16 *mask = lo ? a.mask0 : a.mask1;
-                const int cc = lo ? a.split : a.cout - a.split, ci = lo ? co : co - a.split;
-                if (mask) {
-                    const bf162 mk = *reinterpret_cast<const bf162 *>(mask + pix * cc + ci);
-                    if (!(__low2float(mk) > 0.f))
-                        v0 = 0.f;
-                    if (!(__high2float(mk) > 0.f))
-                        v1 = 0.f;
-                }
-                *reinterpret_cast<bf162 *>(dst + pix * cc + ci) = __floats2bfloat162_rn(v0, v1);
             }
         }
     }
@@ -281,7 +377,7 @@ __host__ __device__ constexpr uint32_t instr_desc_bf16_mn(int n)
 template <int NW, int NST>
 __global__ void __launch_bounds__(128) k_conv3x3_wgrad_umma(WgradArgs a, int slabs_per_cta)
 {
-    extern __shared__ __align__(128) unsigned char smu[];
+    extern __shared__ __align__(1024) unsigned char smu[];
     constexpr int SB = umma_wg_stage_bytes(NW);
     constexpr uint32_t NCOLS = 9 * NW <= 256 ? 256u : 512u;
     uint64_t *bar = reinterpret_cast<uint64_t *>(smu + NST * SB);

@@ -176,20 +176,38 @@ class UNet:
         return B
 
     # ---- primitives -------------------------------------------------------
+    # optional per-launch timing of the convolutions: a list that receives
+    # (kind, layer, flop, start event, end event) per call, or None
+    timers = None
+
+    def _timed(self, kind, name, flop, launch):
+        if self.timers is None:
+            return launch()
+        import torch
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.current_stream(self.dev)  # the stream the kernels are launched on (_stream)
+        e0.record(st)
+        rc = launch()
+        e1.record(st)
+        self.timers.append((kind, name, flop, e0, e1))
+        return rc
+
     def _conv(self, name, src0, dst, N, H, W, src1=None, up1=0, relu=1):
         _, cin, cout = next(l for l in self.layers if l[0] == name)
         c0 = src0.shape[-1]
         c1 = 0 if src1 is None else src1.shape[-1]
         assert c0 + c1 == cin
-        self._ok(self.L.otf_unet_conv3x3(_p(src0), c0, _p(src1), c1, up1, _p(self.wf[name]), _p(self.bias(name)),
-                                         relu, _p(dst), None, None, None, cout, cout, N, H, W, self._stream()))
+        self._ok(self._timed("fwd", name, 18.0 * cin * cout * N * H * W, lambda: self.L.otf_unet_conv3x3(
+            _p(src0), c0, _p(src1), c1, up1, _p(self.wf[name]), _p(self.bias(name)), relu, _p(dst), None, None,
+            None, cout, cout, N, H, W, self._stream())))
 
     def _dgrad(self, name, dz, dst0, mask0, N, H, W, dst1=None, split=None):
         """input gradient of conv `name` from its pre-activation gradient dz."""
         _, cin, cout = next(l for l in self.layers if l[0] == name)
         split = cin if split is None else split
-        self._ok(self.L.otf_unet_conv3x3(_p(dz), cout, None, 0, 0, _p(self.wb[name]), None, 0, _p(dst0),
-                                         _p(mask0), _p(dst1), None, split, cin, N, H, W, self._stream()))
+        self._ok(self._timed("dgrad", name, 18.0 * cin * cout * N * H * W, lambda: self.L.otf_unet_conv3x3(
+            _p(dz), cout, None, 0, 0, _p(self.wb[name]), None, 0, _p(dst0), _p(mask0), _p(dst1), None, split, cin,
+            N, H, W, self._stream())))
 
     def _wgrad(self, name, src0, dz, N, H, W, src1=None, up1=0):
         _, cin, cout = next(l for l in self.layers if l[0] == name)
@@ -197,8 +215,8 @@ class UNet:
         c1 = 0 if src1 is None else src1.shape[-1]
         a, b = self.offsets[name]
         st = self._stream()
-        self._ok(self.L.otf_unet_conv3x3_wgrad(_p(src0), c0, _p(src1), c1, up1, _p(dz), cout,
-                                               _p(self.grads[a:b]), N, H, W, self.sm, st))
+        self._ok(self._timed("wgrad", name, 18.0 * cin * cout * N * H * W, lambda: self.L.otf_unet_conv3x3_wgrad(
+            _p(src0), c0, _p(src1), c1, up1, _p(dz), cout, _p(self.grads[a:b]), N, H, W, self.sm, st)))
         self._ok(self.L.otf_unet_bias_grad(_p(dz), cout, N * H * W, _p(self.grads[b:b + cout]), st))
 
     # ---- network ----------------------------------------------------------
@@ -324,9 +342,14 @@ def _bench(argv=None):
     ap.add_argument("--hw", type=int, default=256)
     ap.add_argument("--iters", type=int, default=10)
     ap.add_argument("--legacy", action="store_true", help="warp-level mma.sync convolutions instead of tcgen05")
+    ap.add_argument("--tcgen05-all", action="store_true",
+                    help="tcgen05 for every layer's weight gradient too (by default small layers keep mma.sync)")
+    ap.add_argument("--convs", action="store_true",
+                    help="also time every 3x3 convolution launch of a training step (forward, input gradient, "
+                         "weight gradient) and report TFLOP/s per kind and per layer")
     a = ap.parse_args(argv)
     net = UNet(base=32)
-    net.L.otf_unet_set_umma(0 if a.legacy else 1)
+    net.L.otf_unet_set_umma(0 if a.legacy else (2 if a.tcgen05_all else 1))
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
     x = torch.randn(a.n, a.hw, a.hw, 3, device="cuda", generator=g)
@@ -353,10 +376,31 @@ def _bench(argv=None):
     for name, cin, cout in net.layers:
         lvl = {"enc1": 0, "dec1": 0, "enc2": 1, "dec2": 1, "enc3": 2, "dec3": 2, "bota": 3, "botb": 3}[name[:4]]
         flop += 2.0 * 9 * cin * cout * a.n * (a.hw >> lvl) ** 2
-    status = int(net.L.otf_unet_status())
-    print(json.dumps({"n": a.n, "hw": a.hw, "conv": "mma.sync" if a.legacy else "tcgen05",
-                      "forward_ms": f_ms, "forward_tflops": flop / f_ms / 1e9,
-                      "train_step_ms": s_ms, "train_tflops": 3 * flop / s_ms / 1e9, "device_status": status}))
+    out = {"n": a.n, "hw": a.hw, "conv": "mma.sync" if a.legacy else ("tcgen05 (all)" if a.tcgen05_all else "tcgen05"),
+           "forward_ms": f_ms, "forward_tflops": flop / f_ms / 1e9,
+           "train_step_ms": s_ms, "train_tflops": 3 * flop / s_ms / 1e9}
+    if a.convs:
+        # per-launch events around each convolution of a few training steps
+        # (the launches run back to back, as in an untimed step)
+        kinds, layers = {}, {}
+        for _ in range(a.iters):
+            net.timers = []
+            net.train_step(x, t)
+            torch.cuda.synchronize()
+            for kind, name, fl, e0, e1 in net.timers:
+                ms = e0.elapsed_time(e1)
+                k = kinds.setdefault(kind, [0.0, 0.0])
+                k[0] += fl
+                k[1] += ms
+                l = layers.setdefault(f"{kind}:{name}", [0.0, 0.0])
+                l[0] += fl
+                l[1] += ms
+        net.timers = None
+        out["conv_tflops"] = {k: v[0] / v[1] / 1e9 for k, v in kinds.items()}
+        out["conv_ms_per_step"] = {k: v[1] / a.iters for k, v in kinds.items()}
+        out["conv_layer_tflops"] = {k: round(v[0] / v[1] / 1e9, 1) for k, v in layers.items()}
+    out["device_status"] = int(net.L.otf_unet_status())
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":

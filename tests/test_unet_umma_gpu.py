@@ -122,7 +122,7 @@ def test_umma_wgrad_vs_oracle_and_legacy(lib, case):
     st = torch.cuda.current_stream().cuda_stream
     res = {}
     for umma in (1, 0):
-        L.otf_unet_set_umma(umma)
+        L.otf_unet_set_umma(2 if umma else 0)  # 2: tcgen05 whatever the layer size
         dW = torch.zeros(9 * cout * cin, dtype=torch.float32, device="cuda")
         assert L.otf_unet_conv3x3_wgrad(_p(X0), c0, _p(X1), c1, up1, _p(DZ), cout, _p(dW), N, H, W, sm, st) == 0
         torch.cuda.synchronize()
