@@ -331,6 +331,42 @@ class UNet:
         return loss
 
 
+def _bench_conv(a):
+    """One forward convolution (bias + ReLU) of the given shape, launched
+    `iters` times after 3 warm-up launches, timed with CUDA events."""
+    import json
+
+    import torch
+    N, H, W, cin, cout = (int(v) for v in a.conv.split(","))
+    L = _declare(_lib.load())
+    L.otf_unet_set_umma(0 if a.legacy else 1)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    x = torch.randn(N, H, W, cin, device="cuda", generator=g).to(torch.bfloat16)
+    w = (torch.randn(9 * cout * cin, device="cuda", generator=g) / (3.0 * cin ** 0.5)).to(torch.bfloat16)
+    b = torch.zeros(cout, device="cuda")
+    y = torch.empty(N, H, W, cout, dtype=torch.bfloat16, device="cuda")
+    st = c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def launch():
+        if L.otf_unet_conv3x3(_p(x), cin, None, 0, 0, _p(w), _p(b), 1, _p(y), None, None, None, cout, cout,
+                              N, H, W, st) != 0:
+            _lib.check(L)
+
+    for _ in range(3):
+        launch()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.iters):
+        launch()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.iters
+    flop = 18.0 * cin * cout * N * H * W
+    print(json.dumps({"conv": [N, H, W, cin, cout], "kernel": "mma.sync" if a.legacy else "tcgen05",
+                      "ms": ms, "tflops": flop / ms / 1e9, "device_status": int(L.otf_unet_status())}))
+
+
 def _bench(argv=None):
     """Time forward and training steps: python -m otfwi_b200.unet --n 16 --hw 256."""
     import argparse
@@ -347,7 +383,11 @@ def _bench(argv=None):
     ap.add_argument("--convs", action="store_true",
                     help="also time every 3x3 convolution launch of a training step (forward, input gradient, "
                          "weight gradient) and report TFLOP/s per kind and per layer")
+    ap.add_argument("--conv", default="",
+                    help="time one forward 3x3 convolution alone instead of the network: N,H,W,cin,cout")
     a = ap.parse_args(argv)
+    if a.conv:
+        return _bench_conv(a)
     net = UNet(base=32)
     net.L.otf_unet_set_umma(0 if a.legacy else (2 if a.tcgen05_all else 1))
     g = torch.Generator(device="cuda")
