@@ -91,12 +91,13 @@ int otf_set_precision(int precision);
 int otf_set_tile(int tile);
 /* Free every buffer of the drop-in state. */
 void otf_release(void);
-/* Exercises the failure reporting of the paired step kernels' device-side
- * synchronisation without any GPU fault: one bounded wait on a counter that
- * nothing increments (it gives up after its 0.5 s limit) and one check of a
- * ticket count against a wrong expectation. Writes the error bits the device
- * recorded to *bits (2 = a dependency wait timed out, 4 = tickets out of
- * range); returns 0 when both were reported, -1 otherwise. */
+/* Exercises the failure reporting of the step kernels' device-side checks
+ * without any GPU fault: one bounded wait on a counter that nothing
+ * increments (it gives up after its 0.5 s limit), one check of a paired
+ * ticket count and one of an unfused launch count against wrong
+ * expectations. Writes the error bits the device recorded to *bits (2 = a
+ * dependency wait timed out, 4 = tickets out of range, 8 = a time loop's
+ * launches short); returns 0 when all three were reported, -1 otherwise. */
 int otf_selftest_paired_faults(int *bits);
 
 /* ---- Part 3: batched shots (additive) -----------------------------------

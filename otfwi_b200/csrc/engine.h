@@ -245,6 +245,7 @@ class Engine {
     }
     int n_strips_ = 0, seg_h_ = 64;
     int *derr_ = nullptr;         // device error flag of the bounded waits
+    unsigned *ledger_ = nullptr;  // launches of the unfused step kernels in the current time loop
     TmaParams *tmap_ = nullptr;   // tensor maps of every field, slot and coefficient
     bool maps_dirty_ = true;
 };

@@ -59,6 +59,7 @@ namespace otf {
 constexpr int kErrWaitTimeout = 1;    // an mbarrier wait of a TMA kernel timed out
 constexpr int kErrDepTimeout = 2;     // a paired A item's wait for its P items timed out
 constexpr int kErrTicketRange = 4;    // a paired launch saw tickets outside its range
+constexpr int kErrLedger = 8;         // a time loop's unfused launches did not all run
 
 struct PairedParams {
     UnfusedParams U;
@@ -243,6 +244,14 @@ __global__ void __launch_bounds__(kUThreads, MINB) k_paired_rev(const __grid_con
         if (x < p.X)
             a_rev_segment<true>(U, shot, x, sg * kURows);
     }
+}
+
+// After a loop of unfused launches: as many launches counted as issued, or
+// the error flag.
+__global__ void k_ledger_check(const unsigned *ledger, unsigned expect, int *err)
+{
+    if (*ledger != expect)
+        atomicOr(err, kErrLedger);
 }
 
 // After a loop of paired launches: every ticket handed out exactly once (n

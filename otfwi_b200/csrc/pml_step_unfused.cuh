@@ -71,7 +71,17 @@ struct UnfusedParams {
     // (ring id = the caller's ring index)
     const int *rec_off, *ring_off;
     int record_ring;  // forward: also record the boundary ring
+    unsigned *ledger;  // launches of this time loop: the first CTA of each launch counts it
 };
+
+// Count this launch (thread 0 of the first CTA), after pdl_enter: a launch
+// that never ran leaves the count short, which the loop's check turns into
+// an error of the call.
+__device__ __forceinline__ void count_launch(const UnfusedParams &U)
+{
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0u)
+        atomicAdd(U.ledger, 1u);
+}
 
 // Programmatic dependent launch: the engine launches these kernels with
 // programmatic stream serialization, so a kernel's CTAs may be scheduled
@@ -238,6 +248,7 @@ constexpr int kUAMinBlocks = 28;
 __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
+    count_launch(U);
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     const int cta = blockIdx.x + U.ncb * blockIdx.y;
     if (x < U.p.X)
@@ -252,6 +263,7 @@ __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const
 __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_rev(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
+    count_launch(U);
     const StepParams &p = U.p;
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     const int cta = blockIdx.x + U.ncb * blockIdx.y;
@@ -364,6 +376,7 @@ __device__ __forceinline__ void a_fwd_segment(const UnfusedParams &U, int shot, 
 __global__ void __launch_bounds__(kUThreads, kUAMinBlocks) k_unfused_a_fwd(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
+    count_launch(U);
     const StepParams &p = U.p;
     const int shot = (int)(gridDim.z - 1u - blockIdx.z);
     const int64_t so = p.shot_stride * shot;
@@ -496,11 +509,157 @@ __device__ __forceinline__ void a_rev_segment(const UnfusedParams &U, int shot, 
     }
 }
 
+// The reverse A half-step split by field set, for twice the CTAs at a lower
+// register count than a_rev_segment (the same arithmetic, bit for bit):
+// the reconstruction set with the Laplacian of P_rec(t) and the imaging
+// condition (P_adj(t) read on the CTA's own cells) ...
+__device__ __forceinline__ void a_rev_rec_segment(const UnfusedParams &U, int shot, int x, int z0)
+{
+    const StepParams &p = U.p;
+    const int64_t so = p.shot_stride * shot;
+    const float *__restrict__ PR = p.f0.px_out + so;
+    const float *__restrict__ PA = p.f1.px_out + so;
+    const int64_t col = x + PAD, pitch = p.pitch;
+    bool xin[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        xin[j] = x + j >= 4 && x + j < p.X - 4;
+    float wr[4][9];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const float4 v = uld4(PR + (int64_t)(z0 - 4 + k + PAD) * pitch + col);
+        wr[0][k] = v.x;
+        wr[1][k] = v.y;
+        wr[2][k] = v.z;
+        wr[3][k] = v.w;
+    }
+    const int nz = min(kURows, p.Z - z0);
+    for (int r = 0; r < nz; r++) {
+        const int z = z0 + r;
+        const int64_t o = (int64_t)(z + PAD) * pitch + col;
+        const bool zin = z >= 4 && z < p.Z - 4;
+        {
+            const float4 v = uld4(PR + o + 4 * pitch);
+            wr[0][8] = v.x;
+            wr[1][8] = v.y;
+            wr[2][8] = v.z;
+            wr[3][8] = v.w;
+        }
+        float u[12], ax[4], az[4], nx[4], nzv[4], lap[4], pa[4], g[4];
+        f4a(uld4(PR + o - 4), u);
+        f4a(uld4(PR + o), u + 4);
+        f4a(uld4(PR + o + 4), u + 8);
+        f4a(uld4(p.f0.ax_in + so + o), ax);
+        f4a(uld4(p.f0.az_in + so + o), az);
+        f4a(uld4(PA + o), pa);
+        f4a(uld4c(p.grad + so + o), g);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float dx, dz, lx, lz;
+            dstag_n<1>(u + j + 1, &dx);
+            dstag_n<1>(wr[j] + 1, &dz);
+            lap_n<1>(u + j, &lx);
+            lap_n<1>(wr[j], &lz);
+            lap[j] = lap_combine(lx, lz);
+            a_update(p, true, 1.f, 1.f, dx, dz, ax[j], az[j], xin[j] && zin, nx[j], nzv[j]);
+            g[j] = __fmaf_rn(pa[j], lap[j], g[j]);
+        }
+        ust4(p.f0.ax_out + so + o, nx);
+        ust4(p.f0.az_out + so + o, nzv);
+        ust4(p.grad + so + o, g);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                wr[j][k] = wr[j][k + 1];
+    }
+}
+
+// ... and the adjoint set (damped A update).
+__device__ __forceinline__ void a_rev_adj_segment(const UnfusedParams &U, int shot, int x, int z0)
+{
+    const StepParams &p = U.p;
+    const int64_t so = p.shot_stride * shot;
+    const float *__restrict__ PA = p.f1.px_out + so;
+    const int64_t col = x + PAD, pitch = p.pitch;
+    float dmx[4];
+    f4a(uld4(p.dampx + col), dmx);
+    bool xin[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        xin[j] = x + j >= 4 && x + j < p.X - 4;
+    float wa[4][8];
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        const float4 v = uld4(PA + (int64_t)(z0 - 3 + k + PAD) * pitch + col);
+        wa[0][k] = v.x;
+        wa[1][k] = v.y;
+        wa[2][k] = v.z;
+        wa[3][k] = v.w;
+    }
+    const int nz = min(kURows, p.Z - z0);
+#pragma unroll 2
+    for (int r = 0; r < nz; r++) {
+        const int z = z0 + r;
+        const int64_t o = (int64_t)(z + PAD) * pitch + col;
+        const bool zin = z >= 4 && z < p.Z - 4;
+        {
+            const float4 a = uld4(PA + o + 4 * pitch);
+            wa[0][7] = a.x;
+            wa[1][7] = a.y;
+            wa[2][7] = a.z;
+            wa[3][7] = a.w;
+        }
+        float u[12], ax[4], az[4], nx[4], nzv[4];
+        f4a(uld4(PA + o - 4), u);
+        f4a(uld4(PA + o), u + 4);
+        f4a(uld4(PA + o + 4), u + 8);
+        f4a(uld4(p.f1.ax_in + so + o), ax);
+        f4a(uld4(p.f1.az_in + so + o), az);
+        const float dmz = __ldg(p.dampz + z + PAD);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float dx, dz;
+            dstag_n<1>(u + j + 1, &dx);
+            dstag_n<1>(wa[j], &dz);
+            a_update(p, false, dmx[j], dmz, dx, dz, ax[j], az[j], xin[j] && zin, nx[j], nzv[j]);
+        }
+        ust4(p.f1.ax_out + so + o, nx);
+        ust4(p.f1.az_out + so + o, nzv);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int k = 0; k < 7; k++)
+                wa[j][k] = wa[j][k + 1];
+    }
+}
+
+// Reverse A half-steps split by set: grid (ncb, nseg, 2 * n_shots), shot
+// (z / 2) downwards; even z: reconstruction + imaging, odd z: adjoint.
+// Register cap from a sweep (16 / 20 / 24 resident CTAs: 115 / 96 / 80
+// registers, the last spilling): 20 is the fastest.
+constexpr int kUARevMinBlocks = 20;
+template <int MINB>
+__global__ void __launch_bounds__(kUThreads, MINB) k_unfused_a_rev_sets(const __grid_constant__ UnfusedParams U)
+{
+    pdl_enter();
+    count_launch(U);
+    const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
+    if (x >= U.p.X)
+        return;
+    const int shot = (int)(gridDim.z / 2u - 1u - (blockIdx.z >> 1));
+    if ((blockIdx.z & 1u) == 0u)
+        a_rev_rec_segment(U, shot, x, blockIdx.y * kURows);
+    else
+        a_rev_adj_segment(U, shot, x, blockIdx.y * kURows);
+}
+
 // Reverse A half-steps of both sets and the imaging condition: grid (ncb,
 // nseg, n_shots), shots downwards.
 __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
+    count_launch(U);
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= U.p.X)
         return;

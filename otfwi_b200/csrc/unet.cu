@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <cudaTypedefs.h>
@@ -563,6 +564,11 @@ using namespace otf::unet;
 
 namespace {
 int g_use_umma = 1;
+// persistent resident-weight convolution for the small layers (OTFWI_CONV_RES=0: off)
+const bool g_conv_res = [] {
+    const char *v = getenv("OTFWI_CONV_RES");
+    return !(v && v[0] == '0');
+}();
 bool use_umma() { return g_use_umma != 0; }
 
 // Tiled BF16 tensor map (rank 3 or 4, no swizzle, zero fill outside).
@@ -672,10 +678,42 @@ int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1
             if (nb > 256 && cout % c == 0)
                 nb = c;
         const int tiles = ((W + umma::TWU - 1) / umma::TWU) * ((H + umma::TH2 - 1) / umma::TH2) * N;
-        const dim3 grid((unsigned)tiles, (unsigned)(cout / nb));
+        // small images (the bottom of the network): split the output channels
+        // further while fewer CTAs than SMs would run
+        static const int sms = [] {
+            int dev = 0, n = 148;
+            if (cudaGetDevice(&dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+                n = 148;
+            return n;
+        }();
+        // (blocks stay multiples of 32 channels: the epilogues read the
+        // accumulators 32 columns at a time)
+        while (nb > 64 && (int64_t)tiles * (cout / nb) < sms && (nb / 2) % 32 == 0 && cout % (nb / 2) == 0)
+            nb /= 2;
+        OTF_CHECK(nb % 32 == 0 && cout % nb == 0, 1, "conv3x3: internal channel block not a multiple of 32");
         ConvMaps maps;
         if (conv_maps(&maps, a, nb))
             return -1;
+        const int nk = (c0 + c1) / KC;
+        if (g_conv_res && nb <= 128 && 288 * nb * nk <= kResWeightBytes) {
+            // small layer: persistent CTAs with the weights resident
+            const int smem = umma_res_smem_bytes(nb, nk);
+            int ncols = 32;
+            while (ncols < 4 * nb)
+                ncols <<= 1;
+            int cps = (228 * 1024) / (smem + 1024);
+            cps = cps < 512 / ncols ? cps : 512 / ncols;
+            cps = cps < 1 ? 1 : cps;
+            const int ncb = cout / nb;
+            int gx = sms * cps / ncb;
+            gx = gx < 1 ? 1 : (gx > tiles ? tiles : gx);
+            OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_umma_res, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            k_conv3x3_umma_res<<<dim3((unsigned)gx, (unsigned)ncb), 256, smem, (cudaStream_t)stream>>>(a, maps, nb,
+                                                                                                     tiles);
+            return launch_status();
+        }
+        const dim3 grid((unsigned)tiles, (unsigned)(cout / nb));
         const int nst = conv_stages(nb);
         const int smem = umma_smem_bytes(nb, nst);
         auto kern = nst == 2 ? k_conv3x3_umma<2> : nst == 3 ? k_conv3x3_umma<3> : k_conv3x3_umma<4>;

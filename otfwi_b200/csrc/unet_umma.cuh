@@ -7,13 +7,14 @@
 //   K = 9 taps x the input channels, taken 16 channels (one MMA K) at a time.
 //
 // Warp roles, each stage a full / empty mbarrier pair:
-//   warp 0 (producer): per 16-channel chunk, the chunk's weights of every tap
-//     ([tap][cout][8 ch] per 8-channel plane: one 3D TMA load per plane) and
-//     the input halo (34 x 10 pixels x 8 channels per plane: one 4D TMA load
-//     per plane; the tensor map's zero fill supplies the image border); a
-//     chunk of the upsampled second input is gathered by the warp with
-//     cp.async instead (nearest upsampling on load), then made visible to the
-//     tensor cores (fence.proxy.async) before the stage's arrival;
+//   warps 0, 2, 3 (producers): per 16-channel chunk, warp 0 loads the chunk's
+//     weights of every tap ([tap][cout][8 ch] per 8-channel plane: one 3D TMA
+//     load per plane) and the input halo (34 x 10 pixels x 8 channels per
+//     plane: one 4D TMA load per plane; the tensor map's zero fill supplies
+//     the image border); a chunk of the upsampled second input is gathered
+//     by the three warps with cp.async instead (nearest upsampling on load),
+//     then made visible to the tensor cores (fence.proxy.async); each warp
+//     arrives on the stage's full barrier;
 //   warp 1 (one thread): waits for a stage, issues its 18 MMAs (9 taps x 2
 //     halves; kind::f16, BF16 in, FP32 accumulators in tensor memory, 2 x N
 //     columns), and commits them to the stage's empty barrier;
@@ -140,6 +141,105 @@ struct ConvMaps {
 __host__ __device__ constexpr int umma_stage_bytes(int n) { return 2 * umma::PLANE2 + 2 * 9 * n * 16; }
 __host__ __device__ constexpr int umma_smem_bytes(int n, int nst) { return nst * umma_stage_bytes(n) + 256; }
 
+// Epilogue of one 256-pixel tile: the calling warp reads TMEM lanes
+// 32 * quarter .. +31 (one output pixel per lane and half) from the
+// accumulators at column col0 (half h at col0 + h * N), adds the bias,
+// applies the ReLU and the masks, and stores BF16 (16-byte vectors where 8
+// channels lie on one side of the split, aligned).
+__device__ __forceinline__ void conv_epilogue(const ConvArgs &a, uint32_t tmem, uint32_t quarter, int lane,
+                                              uint32_t col0, int N, int n, int y0, int x0, int co0)
+{
+    const int m = (int)quarter * 32 + lane;
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+        const int y = y0 + 16 * h + m / umma::TWU, x = x0 + (m % umma::TWU);
+        const bool inside = y < a.H && x < a.W;
+        const int64_t pix = ((int64_t)n * a.H + y) * a.W + x;
+#pragma unroll 1
+        for (int c0 = 0; c0 < N; c0 += 32) {
+            float v[32];
+            umma::tmem_ld32(tmem + ((quarter * 32u) << 16) + col0 + (uint32_t)(h * N + c0), v);
+            if (!inside)
+                continue;
+#pragma unroll
+            for (int g = 0; g < 32; g += 8) {
+                const int co = co0 + c0 + g;
+                float r[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    r[j] = v[g + j];
+                    if (a.bias)
+                        r[j] += a.bias[co + j];
+                    if (a.relu)
+                        r[j] = fmaxf(r[j], 0.f);
+                }
+                const bool lo = co < a.split;
+                const int cc = lo ? a.split : a.cout - a.split, ci = lo ? co : co - a.split;
+                if (lo == (co + 7 < a.split) && ((cc | ci) & 7) == 0) {
+                    // the 8 channels on one side, 16-byte aligned
+                    bf16 *dst = (lo ? a.dst0 : a.dst1) + pix * cc + ci;
+                    const bf16 *mask = lo ? a.mask0 : a.mask1;
+                    if (mask) {
+                        const uint4 mk = *reinterpret_cast<const uint4 *>(mask + pix * cc + ci);
+                        const bf162 *m2 = reinterpret_cast<const bf162 *>(&mk);
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            if (!(__low2float(m2[j]) > 0.f))
+                                r[2 * j] = 0.f;
+                            if (!(__high2float(m2[j]) > 0.f))
+                                r[2 * j + 1] = 0.f;
+                        }
+                    }
+                    uint4 pk;
+                    bf162 *p2 = reinterpret_cast<bf162 *>(&pk);
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        p2[j] = __floats2bfloat162_rn(r[2 * j], r[2 * j + 1]);
+                    *reinterpret_cast<uint4 *>(dst) = pk;
+                    continue;
+                }
+#pragma unroll
+                for (int j = 0; j < 8; j += 2) {
+                    const int cj = co + j;
+                    float v0 = r[j], v1 = r[j + 1];
+                    const bool l2 = cj < a.split;
+                    bf16 *dst = l2 ? a.dst0 : a.dst1;
+                    const bf16 *mask = l2 ? a.mask0 : a.mask1;
+                    const int c2 = l2 ? a.split : a.cout - a.split, i2 = l2 ? cj : cj - a.split;
+                    if (mask) {
+                        const bf162 mk = *reinterpret_cast<const bf162 *>(mask + pix * c2 + i2);
+                        if (!(__low2float(mk) > 0.f))
+                            v0 = 0.f;
+                        if (!(__high2float(mk) > 0.f))
+                            v1 = 0.f;
+                    }
+                    *reinterpret_cast<bf162 *>(dst + pix * c2 + i2) = __floats2bfloat162_rn(v0, v1);
+                }
+            }
+        }
+    }
+}
+
+// The halo planes of one 16-channel chunk (ch) of a 256-pixel tile, gathered
+// with cp.async (zero fill outside the image; the second input upsampled on
+// load) by `nw` warps, this warp being number `wi`; visible to the tensor
+// cores on return.
+__device__ __forceinline__ void conv_gather(const ConvArgs &a, unsigned char *st, int ch, int n, int y0, int x0,
+                                            int wi, int nw, int lane)
+{
+    for (int i = wi * 32 + lane; i < umma::HPIX2 * 2; i += 32 * nw) {
+        const int px = i >> 1, h = i & 1;
+        const int hy = px / umma::HWU, hx = px - hy * umma::HWU;
+        const int gy = y0 + hy - 1, gx = x0 + hx - 1;
+        const bool in = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
+        const void *src = in ? (const void *)in_ptr(a, n, gy, gx, ch + 8 * h) : (const void *)a.w;
+        cp_async16(reinterpret_cast<uint32_t *>(st + h * umma::PLANE2 + px * 16), src, in ? 16 : 0);
+    }
+    cp_commit();
+    cp_wait<0>();
+    umma::fence_proxy_async();  // cp.async writes -> visible to the tensor cores
+}
+
 template <int NST>
 __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ ConvArgs a,
                                                       const __grid_constant__ ConvMaps maps, int N)
@@ -164,8 +264,10 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ Co
         ncols <<= 1;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < 2 * NST + 1; s++)
-            otf::mbar_init(&full[s], 1);
+        for (int s = 0; s < NST; s++)
+            otf::mbar_init(&full[s], 3);  // one arrival per producer warp
+        for (int s = NST; s < 2 * NST + 1; s++)
+            otf::mbar_init(&full[s], 1);  // empty barriers and `done`: one commit each
         *fail = 0;
         otf::fence_barrier_init();
     }
@@ -176,9 +278,11 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ Co
     umma::fence_after_sync();
     const uint32_t tmem = *tslot;
 
-    if (warp == 0) {
-        // producer
-        if (lane == 0) {
+    if (warp != 1) {
+        // producers: warp 0 issues the TMA loads; warps 0, 2 and 3 share the
+        // cp.async gather of an upsampled chunk; each arrives once per chunk
+        const int pi = warp == 0 ? 0 : warp - 1;
+        if (warp == 0 && lane == 0) {
             otf::tma_prefetch_desc(&maps.w);
             otf::tma_prefetch_desc(&maps.x0);
             if (a.c1 && !a.up1)
@@ -202,7 +306,7 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ Co
             const int ch = kc * KC;
             const bool from1 = ch >= a.c0;
             const bool gather = from1 && a.up1;
-            if (lane == 0) {
+            if (warp == 0 && lane == 0) {
                 otf::mbar_expect_tx(&full[s], wbytes + (gather ? 0u : abytes));
                 for (int h = 0; h < 2; h++)
                     otf::tma_load_3d(st + 2 * umma::PLANE2 + h * 9 * N * 16, &maps.w, ch + 8 * h, co0, 0, &full[s]);
@@ -213,26 +317,15 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ Co
                         otf::tma_load_4d(st + h * umma::PLANE2, mx, c + 8 * h, x0 - 1, y0 - 1, n, &full[s]);
                 }
             }
-            if (gather) {
-                for (int i = lane; i < umma::HPIX2 * 2; i += 32) {
-                    const int px = i >> 1, h = i & 1;
-                    const int hy = px / umma::HWU, hx = px - hy * umma::HWU;
-                    const int gy = y0 + hy - 1, gx = x0 + hx - 1;
-                    const bool in = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
-                    const void *src = in ? (const void *)in_ptr(a, n, gy, gx, ch + 8 * h) : (const void *)a.w;
-                    cp_async16(reinterpret_cast<uint32_t *>(st + h * umma::PLANE2 + px * 16), src, in ? 16 : 0);
-                }
-                cp_commit();
-                cp_wait<0>();
-                umma::fence_proxy_async();  // cp.async writes -> visible to the tensor cores
-            }
+            if (gather)
+                conv_gather(a, st, ch, n, y0, x0, pi, 3, lane);
             __syncwarp();
             if (lane == 0)
                 otf::mbar_arrive(&full[s]);
             issued = kc + 1;
         }
-        // wait for every copy this warp issued (the last fill of each stage)
-        if (lane == 0)
+        // wait for every copy the producers issued (the last fill of each stage)
+        if (warp == 0 && lane == 0)
             for (int kc = issued > NST ? issued - NST : 0; kc < issued; kc++)
                 otf::mbar_wait(&full[kc % NST], (uint32_t)((kc / NST) & 1), &g_unet_err);
         __syncwarp();
@@ -270,80 +363,218 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ Co
     const bool ok = otf::mbar_wait(done, 0, &g_unet_err) && *fail == 0;
     umma::fence_after_sync();
 
-    if (ok) {
-        const int m = warp * 32 + lane;
-#pragma unroll 1
-        for (int h = 0; h < 2; h++) {
-            const int y = y0 + 16 * h + m / umma::TWU, x = x0 + (m % umma::TWU);
-            const bool inside = y < a.H && x < a.W;
-            const int64_t pix = ((int64_t)n * a.H + y) * a.W + x;
-#pragma unroll 1
-            for (int c0 = 0; c0 < N; c0 += 32) {
-                float v[32];
-                umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * N + c0), v);
-                if (!inside)
-                    continue;
-#pragma unroll
-                for (int g = 0; g < 32; g += 8) {
-                    const int co = co0 + c0 + g;
-                    float r[8];
-#pragma unroll
-                    for (int j = 0; j < 8; j++) {
-                        r[j] = v[g + j];
-                        if (a.bias)
-                            r[j] += a.bias[co + j];
-                        if (a.relu)
-                            r[j] = fmaxf(r[j], 0.f);
-                    }
-                    const bool lo = co < a.split;
-                    const int cc = lo ? a.split : a.cout - a.split, ci = lo ? co : co - a.split;
-                    if (lo == (co + 7 < a.split) && ((cc | ci) & 7) == 0) {
-                        // the 8 channels on one side, 16-byte aligned
-                        bf16 *dst = (lo ? a.dst0 : a.dst1) + pix * cc + ci;
-                        const bf16 *mask = lo ? a.mask0 : a.mask1;
-                        if (mask) {
-                            const uint4 mk = *reinterpret_cast<const uint4 *>(mask + pix * cc + ci);
-                            const bf162 *m2 = reinterpret_cast<const bf162 *>(&mk);
-#pragma unroll
-                            for (int j = 0; j < 4; j++) {
-                                if (!(__low2float(m2[j]) > 0.f))
-                                    r[2 * j] = 0.f;
-                                if (!(__high2float(m2[j]) > 0.f))
-                                    r[2 * j + 1] = 0.f;
-                            }
-                        }
-                        uint4 pk;
-                        bf162 *p2 = reinterpret_cast<bf162 *>(&pk);
-#pragma unroll
-                        for (int j = 0; j < 4; j++)
-                            p2[j] = __floats2bfloat162_rn(r[2 * j], r[2 * j + 1]);
-                        *reinterpret_cast<uint4 *>(dst) = pk;
-                        continue;
-                    }
-#pragma unroll
-                    for (int j = 0; j < 8; j += 2) {
-                        const int cj = co + j;
-                        float v0 = r[j], v1 = r[j + 1];
-                        const bool l2 = cj < a.split;
-                        bf16 *dst = l2 ? a.dst0 : a.dst1;
-                        const bf16 *mask = l2 ? a.mask0 : a.mask1;
-                        const int c2 = l2 ? a.split : a.cout - a.split, i2 = l2 ? cj : cj - a.split;
-                        if (mask) {
-                            const bf162 mk = *reinterpret_cast<const bf162 *>(mask + pix * c2 + i2);
-                            if (!(__low2float(mk) > 0.f))
-                                v0 = 0.f;
-                            if (!(__high2float(mk) > 0.f))
-                                v1 = 0.f;
-                        }
-                        *reinterpret_cast<bf162 *>(dst + pix * c2 + i2) = __floats2bfloat162_rn(v0, v1);
-                    }
-                }
-            }
-        }
-    }
+    if (ok)
+        conv_epilogue(a, tmem, (uint32_t)warp, lane, 0u, N, n, y0, x0, co0);
     umma::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(tmem, ncols);
+    }
+}
+
+// Persistent form for the small layers (the CTA's output channels N <= 128
+// and all of its weights within kResWeightBytes): the weights of every chunk
+// and tap stay in shared memory for the CTA's life (one TMA load per chunk
+// and plane at the start, then only halo tiles stream); the CTA walks
+// 256-pixel tiles blockIdx.x, + gridDim.x, ...; two accumulator buffers (2 x
+// 2N tensor-memory columns) let the epilogue of one tile overlap the MMAs of
+// the next. Warps: 0 producer (halo TMA loads; with warps 6 and 7 the
+// cp.async gather of an upsampled chunk), 1 the MMA issuer (one thread),
+// 2-5 the epilogue (TMEM lane quarters 2, 3, 0, 1). Per halo stage a full
+// (three producer warps) / empty (MMA commit) barrier pair; per accumulator
+// buffer a full (MMA commit) / empty (four epilogue warps) pair. Bounded
+// waits as the kernel above; a failed wait sets the error flag, the role
+// stops, and teardown waits (bounded) for the MMAs and copies issued.
+constexpr int kResWeightBytes = 96 * 1024;
+constexpr int kResStages = 4;
+__host__ __device__ constexpr int umma_res_smem_bytes(int n, int nk)
+{
+    return nk * 2 * 9 * n * 16 + kResStages * 2 * umma::PLANE2 + 256;
+}
+
+__global__ void __launch_bounds__(256) k_conv3x3_umma_res(const __grid_constant__ ConvArgs a,
+                                                          const __grid_constant__ ConvMaps maps, int N, int n_tiles)
+{
+    extern __shared__ __align__(1024) unsigned char smu[];
+    constexpr int NST = kResStages;
+    const int cin = a.c0 + a.c1, nk = cin / KC;
+    const int wchunk = 2 * 9 * N * 16;          // bytes of one chunk's weights (two planes)
+    unsigned char *wsm = smu;                   // [chunk][plane][tap][co][8 ch]
+    unsigned char *hsm = smu + nk * wchunk;     // NST halo stages of two planes
+    constexpr int SA = 2 * umma::PLANE2;
+    uint64_t *full = reinterpret_cast<uint64_t *>(hsm + NST * SA);
+    uint64_t *empty = full + NST;
+    uint64_t *acc_full = empty + NST;
+    uint64_t *acc_empty = acc_full + 2;
+    uint64_t *wbar = acc_empty + 2;
+    uint64_t *done = wbar + 1;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
+    int *fail = reinterpret_cast<int *>(tslot + 1);
+    const int tiles_x = (a.W + umma::TWU - 1) / umma::TWU, tiles_y = (a.H + umma::TH2 - 1) / umma::TH2;
+    const int co0 = blockIdx.y * N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int my_tiles = (int)blockIdx.x < n_tiles ? (n_tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    uint32_t ncols = 32;
+    while (ncols < 4u * (uint32_t)N)
+        ncols <<= 1;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NST; i++) {
+            otf::mbar_init(&full[i], 3);   // one arrival per producer warp
+            otf::mbar_init(&empty[i], 1);  // one MMA commit
+        }
+        for (int i = 0; i < 2; i++) {
+            otf::mbar_init(&acc_full[i], 1);   // one MMA commit
+            otf::mbar_init(&acc_empty[i], 4);  // one arrival per epilogue warp
+        }
+        otf::mbar_init(wbar, 1);
+        otf::mbar_init(done, 1);
+        *fail = 0;
+        otf::fence_barrier_init();
+    }
+    if (warp == 0)
+        umma::tmem_alloc(tslot, ncols);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    auto origin = [&](int li, int &n, int &y0, int &x0) {
+        int t = (int)blockIdx.x + li * (int)gridDim.x;
+        n = t / (tiles_x * tiles_y);
+        t -= n * tiles_x * tiles_y;
+        const int ty = t / tiles_x;
+        y0 = ty * umma::TH2;
+        x0 = (t - ty * tiles_x) * umma::TWU;
+    };
+
+    if (warp == 0 || warp >= 6) {
+        // producers
+        const int pi = warp == 0 ? 0 : warp - 5;
+        if (warp == 0 && lane == 0) {
+            otf::tma_prefetch_desc(&maps.w);
+            otf::tma_prefetch_desc(&maps.x0);
+            if (a.c1 && !a.up1)
+                otf::tma_prefetch_desc(&maps.x1);
+            otf::mbar_arrive_expect_tx(wbar, (uint32_t)(nk * wchunk));
+            for (int kc = 0; kc < nk; kc++)
+                for (int h = 0; h < 2; h++)
+                    otf::tma_load_3d(wsm + kc * wchunk + h * 9 * N * 16, &maps.w, kc * KC + 8 * h, co0, 0, wbar);
+        }
+        const uint32_t abytes = 2u * umma::HPIX2 * 16u;
+        int g = 0;
+        bool ok = true;
+        for (int li = 0; li < my_tiles && ok; li++) {
+            int n, y0, x0;
+            origin(li, n, y0, x0);
+            for (int kc = 0; kc < nk; kc++, g++) {
+                const int s = g % NST;
+                if (g >= NST) {
+                    int okw = 1;
+                    if (lane == 0)
+                        okw = otf::mbar_wait(&empty[s], (uint32_t)((g / NST - 1) & 1), &g_unet_err) ? 1 : 0;
+                    if (!__shfl_sync(0xffffffffu, okw, 0)) {
+                        if (lane == 0)
+                            *fail = 1;
+                        ok = false;
+                        break;
+                    }
+                }
+                unsigned char *st = hsm + s * SA;
+                const int ch = kc * KC;
+                const bool from1 = ch >= a.c0;
+                const bool gather = from1 && a.up1;
+                if (warp == 0 && lane == 0 && !gather) {
+                    otf::mbar_expect_tx(&full[s], abytes);
+                    const CUtensorMap *mx = from1 ? &maps.x1 : &maps.x0;
+                    const int c = from1 ? ch - a.c0 : ch;
+                    for (int h = 0; h < 2; h++)
+                        otf::tma_load_4d(st + h * umma::PLANE2, mx, c + 8 * h, x0 - 1, y0 - 1, n, &full[s]);
+                }
+                if (gather)
+                    conv_gather(a, st, ch, n, y0, x0, pi, 3, lane);
+                __syncwarp();
+                if (lane == 0)
+                    otf::mbar_arrive(&full[s]);
+            }
+        }
+        // wait for every copy issued: the weights and the last fill of each stage
+        if (warp == 0 && lane == 0) {
+            otf::mbar_wait(wbar, 0, &g_unet_err);
+            for (int gg = g > NST ? g - NST : 0; gg < g; gg++)
+                otf::mbar_wait(&full[gg % NST], (uint32_t)((gg / NST) & 1), &g_unet_err);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = umma::instr_desc_bf16(N);
+            bool ok = otf::mbar_wait(wbar, 0, &g_unet_err);
+            int g = 0;
+            for (int li = 0; li < my_tiles && ok; li++) {
+                const int ab = li & 1;
+                if (li >= 2 && !otf::mbar_wait(&acc_empty[ab], (uint32_t)(((li >> 1) - 1) & 1), &g_unet_err)) {
+                    ok = false;
+                    break;
+                }
+                umma::fence_after_sync();
+                const uint32_t d = tmem + (uint32_t)(ab * 2 * N);
+                for (int kc = 0; kc < nk; kc++, g++) {
+                    const int s = g % NST;
+                    if (!otf::mbar_wait(&full[s], (uint32_t)((g / NST) & 1), &g_unet_err)) {
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_after_sync();
+                    const uint32_t abase = otf::smem_u32(hsm + s * SA);
+                    const uint32_t bbase = otf::smem_u32(wsm + kc * wchunk);
+#pragma unroll
+                    for (int tap = 0; tap < 9; tap++) {
+                        const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+                        const uint64_t bd = umma::smem_desc(bbase + tap * N * 16, 9 * N * 16, 128);
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const uint64_t ad = umma::smem_desc(abase + ((dy + 16 * h) * umma::HWU + dx) * 16,
+                                                                umma::PLANE2, umma::HWU * 16);
+                            umma::mma_bf16(d + (uint32_t)(h * N), ad, bd, idesc, kc > 0 || tap > 0);
+                        }
+                    }
+                    umma::mma_commit(&empty[s]);
+                }
+                if (!ok)
+                    break;
+                umma::mma_commit(&acc_full[ab]);
+            }
+            if (!ok)
+                *fail = 1;
+            umma::mma_commit(done);  // arrives once every MMA issued has completed
+        }
+        __syncwarp();
+    } else {
+        // epilogue: warps 2-5, TMEM lane quarter warp % 4
+        const uint32_t quarter = (uint32_t)(warp & 3);
+        for (int li = 0; li < my_tiles; li++) {
+            const int ab = li & 1;
+            const bool okl = otf::mbar_wait(&acc_full[ab], (uint32_t)((li >> 1) & 1), &g_unet_err);
+            if (!__all_sync(0xffffffffu, okl)) {
+                if (lane == 0)
+                    *fail = 1;
+                break;
+            }
+            umma::fence_after_sync();
+            int n, y0, x0;
+            origin(li, n, y0, x0);
+            conv_epilogue(a, tmem, quarter, lane, (uint32_t)(ab * 2 * N), N, n, y0, x0, co0);
+            umma::fence_before_sync();
+            __syncwarp();
+            if (lane == 0)
+                otf::mbar_arrive(&acc_empty[ab]);
+        }
+    }
+    __syncthreads();
+    // teardown: every MMA issued has completed before the tensor memory is freed
+    if (warp == 0) {
+        otf::mbar_wait(done, 0, &g_unet_err);
         umma::fence_after_sync();
         umma::tmem_dealloc(tmem, ncols);
     }

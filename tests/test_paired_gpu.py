@@ -134,9 +134,10 @@ def test_fast_gradient_same_with_and_without_pdl(lib, tmp_path):
 
 
 def test_paired_fault_reporting(lib):
-    """A dependency wait that nothing satisfies gives up after its bound and
-    a ticket count that does not match is flagged: both reach the host as
-    error bits, and the device keeps running work afterwards."""
+    """A dependency wait that nothing satisfies gives up after its bound, and
+    a paired ticket count and an unfused launch count that do not match are
+    flagged: all three reach the host as error bits, and the device keeps
+    running work afterwards."""
     import ctypes
     from otfwi_b200 import _lib
     f = lib.otf_selftest_paired_faults
@@ -145,7 +146,7 @@ def test_paired_fault_reporting(lib):
     bits = ctypes.c_int(0)
     rc = f(ctypes.byref(bits))
     assert rc == 0, (bits.value, lib.otf_last_error())
-    assert bits.value & 2 and bits.value & 4
+    assert bits.value & 2 and bits.value & 4 and bits.value & 8
     sc = _fmc_small(X=160, Z=96, T=120, n=4)
     out = _batch_run(sc, 5)
     assert np.abs(out[2]).max() > 0

@@ -115,14 +115,15 @@ def test_network_forward_and_gradients_vs_oracle(lib):
     gc["c1"] = np.concatenate([gc["e1"], ora.up(gc["d2"])], axis=-1)
     for label, g, tol in (("same activations", ora.backward(gc, B["dout"].cpu().numpy().astype(np.float64)), 1e-2),
                           ("end to end", ora.backward(cache, dout), 8e-2)):
-        worst = 0.0
+        worst, per = 0.0, {}
         for name, cin, cout in uo.layer_table(32):
             a, b = net.offsets[name]
             rw = _rel(got[a:b], g[name][0].ravel())
             rb = _rel(got[b:b + cout], g[name][1])
+            per[name] = (f"{rw:.1e}", f"{rb:.1e}")
             worst = max(worst, rw, rb)
         rh = _rel(got[net.head_off:net.head_off + 33], np.concatenate([g["head"][0], g["head"][1]]))
-        print(label, "worst layer rel L2", worst, "head", rh)
+        print(label, "worst layer rel L2", worst, "head", rh, "per layer (weights, bias)", per)
         assert worst <= tol and rh <= tol
 
 

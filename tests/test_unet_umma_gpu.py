@@ -2,7 +2,8 @@
 cores (k_conv3x3_umma, k_conv3x3_wgrad_umma: the default paths of
 otf_unet_conv3x3 / otf_unet_conv3x3_wgrad) against the numpy oracle (FP64
 sums of the same BF16 operands) and against the warp-level mma.sync kernels
-they replaced, over the shapes the network uses and edge shapes: every
+they replaced (the small layers through the persistent kernel with resident
+weights), over the shapes the network uses and edge shapes: every
 output channel count of the network (32, 64, 128, 256), 96, and 512 (two
 blocks of 256 channels), grids that are not multiples of the 8 x 16 pixel
 tile, the upsampled second input, bias + ReLU and split masked outputs (the
@@ -41,6 +42,12 @@ CASES = [
     (1, 16, 16, 128, 0, 0, 256, 256, False, 0),
     (1, 8, 16, 256, 0, 0, 512, 256, False, 1),    # two 256-channel blocks
     (3, 9, 11, 48, 0, 0, 96, 96, False, 1),       # ragged tiles, cout 96
+    # small layers (persistent kernel, weights resident in shared memory)
+    (2, 24, 40, 32, 32, 1, 32, 32, False, 1),     # concat + upsample
+    (1, 20, 36, 32, 0, 0, 64, 32, True, 0),       # split masked output, no ReLU
+    (5, 40, 24, 16, 0, 0, 32, 32, False, 1),      # ragged last tile row (40 = 32 + 8)
+    (1, 16, 16, 32, 0, 0, 192, 64, True, 0),      # few tiles: 192 channels split into 96-channel blocks,
+                                                  # the split inside the first block (input-gradient form)
 ]
 
 
@@ -94,6 +101,36 @@ def test_umma_conv_vs_oracle_and_legacy(lib, case):
     assert _rel(outs[1][0], outs[0][0]) <= 5e-3
     if split < cout:
         assert _rel(outs[1][1], outs[0][1]) <= 5e-3
+
+
+def test_umma_conv_persistent_many_tiles(lib):
+    """A full-size first layer (16 x 256^2, 32 -> 32 channels): 4096 tiles,
+    so each persistent CTA walks several tiles through both accumulator
+    buffers; against the mma.sync kernel (relative L2 <= 5e-3)."""
+    import torch
+    from otfwi_b200.unet import _declare, _p
+    L = _declare(lib)
+    N, H, W, c, cout = 16, 256, 256, 32, 32
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    X = torch.randn(N, H, W, c, device="cuda", generator=g).to(torch.bfloat16)
+    Wt = (torch.randn(9 * cout * c, device="cuda", generator=g) / 17.0).to(torch.bfloat16)
+    B = torch.randn(cout, device="cuda", generator=g)
+    st = torch.cuda.current_stream().cuda_stream
+    outs = {}
+    for umma in (1, 0):
+        L.otf_unet_set_umma(umma)
+        D = torch.full((N, H, W, cout), float("nan"), dtype=torch.bfloat16, device="cuda")
+        assert L.otf_unet_conv3x3(_p(X), c, None, 0, 0, _p(Wt), _p(B), 1, _p(D), None, None, None, cout, cout,
+                                  N, H, W, st) == 0, lib.otf_last_error()
+        torch.cuda.synchronize()
+        outs[umma] = D.float()
+    L.otf_unet_set_umma(1)
+    assert L.otf_unet_status() == 0
+    assert torch.isfinite(outs[1]).all()
+    e = float(torch.linalg.vector_norm(outs[1] - outs[0]) / torch.linalg.vector_norm(outs[0]))
+    print(f"persistent 16x256^2 32->32: rel L2 vs mma.sync {e:.2e}")
+    assert e <= 5e-3
 
 
 WG_CASES = [
