@@ -258,6 +258,17 @@ int otf_misfit_noalloc(int kind, const float *sim, const float *obs, float *adj,
 int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1, const void *w,
                      const float *bias, int relu, void *dst0, const void *mask0, void *dst1,
                      const void *mask1, int split, int cout, int N, int H, int W, void *stream);
+/* As otf_unet_conv3x3, with the weights also given packed for the tcgen05
+ * kernels (wp, from otf_unet_pack_weights_tc of w): their stages then load
+ * the weights by contiguous bulk copies instead of 16-byte tiled rows. */
+int otf_unet_conv3x3_packed(const void *src0, int c0, const void *src1, int c1, int up1, const void *w,
+                            const void *wp, const float *bias, int relu, void *dst0, const void *mask0,
+                            void *dst1, const void *mask1, int split, int cout, int N, int H, int W,
+                            void *stream);
+/* wp [cin/8][9][cout][8] (BF16) = w [9][cout][cin] (BF16) regrouped by
+ * 8-channel plane, the layout otf_unet_conv3x3_packed takes; cin a multiple
+ * of 16. */
+int otf_unet_pack_weights_tc(const void *w, int cout, int cin, void *wp, void *stream);
 /* dw [9][cout][c0+c1] (FP32) += weight gradient for the pre-activation
  * gradient dz [N][H][W][cout] of that convolution's inputs. */
 int otf_unet_conv3x3_wgrad(const void *src0, int c0, const void *src1, int c1, int up1, const void *dz,

@@ -20,6 +20,7 @@
 // backward cost no extra pass.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -47,6 +48,7 @@ struct ConvArgs {
     const bf16 *src0, *src1;  // input channels [0, c0) from src0, [c0, c0+c1) from src1
     int c0, c1, up1;          // up1: src1 has half the resolution (nearest upsampling)
     const bf16 *w;            // [9][cout][c0+c1]
+    const bf16 *wp;           // tcgen05 kernels: the same weights packed [(c0+c1)/8][9][cout][8]
     const float *bias;        // [cout] or null
     int relu;
     bf16 *dst0, *dst1;        // channels [0, split) -> dst0, [split, cout) -> dst1
@@ -564,9 +566,10 @@ using namespace otf::unet;
 
 namespace {
 int g_use_umma = 1;
-// persistent resident-weight convolution for the small layers (OTFWI_CONV_RES=0: off)
-const bool g_conv_res = [] {
-    const char *v = getenv("OTFWI_CONV_RES");
+// persistent convolution for the layers with <= 128 output channels per CTA
+// (OTFWI_CONV_PERSISTENT=0: the one-tile kernel for every layer)
+const bool g_conv_pers = [] {
+    const char *v = getenv("OTFWI_CONV_PERSISTENT");
     return !(v && v[0] == '0');
 }();
 bool use_umma() { return g_use_umma != 0; }
@@ -591,17 +594,18 @@ int encode_bf16_map(CUtensorMap *m, const void *base, int rank, const cuuint64_t
     return 0;
 }
 
-// The maps of k_conv3x3_umma: weights (cin, cout, 9) with box (8, nb, 9);
-// the inputs (c, W, H, N) with box (8, 10, 34, 1).
+// The maps of the tcgen05 convolutions: the weights (cin, cout, 9) with box
+// (8, nb, 9) when no packed copy is given; the inputs (c, W, H, N) with box
+// (8, 10, 34, 1).
 int conv_maps(ConvMaps *m, const ConvArgs &a, int nb)
 {
     std::memset(m, 0, sizeof(*m));
-    const int cin = a.c0 + a.c1;
-    {
+    if (!a.wp) {
+        const int cin = a.c0 + a.c1;
         const cuuint64_t dims[3] = {(cuuint64_t)cin, (cuuint64_t)a.cout, 9};
         const cuuint64_t str[2] = {(cuuint64_t)cin * 2, (cuuint64_t)a.cout * cin * 2};
-        const cuuint32_t box[3] = {8, (cuuint32_t)nb, 9};
-        if (encode_bf16_map(&m->w, a.w, 3, dims, str, box))
+        const cuuint32_t wbox[3] = {8, (cuuint32_t)nb, 9};
+        if (encode_bf16_map(&m->w, a.w, 3, dims, str, wbox))
             return -1;
     }
     const cuuint32_t box[4] = {8, (cuuint32_t)umma::HWU, (cuuint32_t)umma::HH2, 1};
@@ -638,13 +642,53 @@ int launch_status()
     }
     return 0;
 }
+// Launch of the tcgen05 convolution for channel blocks of nb (the weights
+// already packed in a.wp): the persistent kernel for nb <= 128, else the
+// one-tile kernel.
+int conv_umma_launch(const ConvArgs &a, const ConvMaps &maps, int nb, int nk, int tiles, cudaStream_t st)
+{
+    const int cout = a.cout;
+    static const int sms = [] {
+        int dev = 0, n = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            n = 148;
+        return n;
+    }();
+    if (g_conv_pers && nb <= 128 && 288 * nb * nk <= kResWeightBytes) {
+        // the small layers: persistent CTAs with the weights resident and
+        // double-buffered accumulators (with the weights streamed instead,
+        // the persistent form measured slower than one tile per CTA)
+        const int smem = umma_res_smem_bytes(nb, nk);
+        int ncols = 32;
+        while (ncols < 4 * nb)
+            ncols <<= 1;
+        int cps = (228 * 1024) / (smem + 1024);
+        cps = cps < 512 / ncols ? cps : 512 / ncols;
+        cps = cps < 1 ? 1 : cps;
+        const int ncb = cout / nb;
+        int gx = sms * cps / ncb;
+        gx = gx < 1 ? 1 : (gx > tiles ? tiles : gx);
+        auto kern = k_conv3x3_umma_pers<true, kResStages>;
+        OTF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        kern<<<dim3((unsigned)gx, (unsigned)ncb), 256, smem, st>>>(a, maps, nb, tiles);
+        return launch_status();
+    }
+    const dim3 grid((unsigned)tiles, (unsigned)(cout / nb));
+    const int nst = conv_stages(nb);
+    const int smem = umma_smem_bytes(nb, nst);
+    auto kern = nst == 2 ? k_conv3x3_umma<2> : nst == 3 ? k_conv3x3_umma<3> : k_conv3x3_umma<4>;
+    OTF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    kern<<<grid, 128, smem, st>>>(a, maps, nb);
+    return launch_status();
+}
 }  // namespace
 
 extern "C" {
 
-int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1, const void *w,
-                     const float *bias, int relu, void *dst0, const void *mask0, void *dst1,
-                     const void *mask1, int split, int cout, int N, int H, int W, void *stream)
+int otf_unet_conv3x3_packed(const void *src0, int c0, const void *src1, int c1, int up1, const void *w,
+                            const void *wp, const float *bias, int relu, void *dst0, const void *mask0, void *dst1,
+                            const void *mask1, int split, int cout, int N, int H, int W, void *stream)
 {
     OTF_CHECK(c0 % 16 == 0 && c1 % 16 == 0 && c0 + c1 > 0 && cout % BN == 0, 1,
               "conv3x3: channel counts must be multiples of 16 (input) and 32 (output)");
@@ -659,6 +703,7 @@ int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1
     a.c1 = c1;
     a.up1 = up1;
     a.w = (const bf16 *)w;
+    a.wp = (const bf16 *)wp;
     a.bias = bias;
     a.relu = relu;
     a.dst0 = (bf16 *)dst0;
@@ -696,33 +741,27 @@ int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1
         if (conv_maps(&maps, a, nb))
             return -1;
         const int nk = (c0 + c1) / KC;
-        if (g_conv_res && nb <= 128 && 288 * nb * nk <= kResWeightBytes) {
-            // small layer: persistent CTAs with the weights resident
-            const int smem = umma_res_smem_bytes(nb, nk);
-            int ncols = 32;
-            while (ncols < 4 * nb)
-                ncols <<= 1;
-            int cps = (228 * 1024) / (smem + 1024);
-            cps = cps < 512 / ncols ? cps : 512 / ncols;
-            cps = cps < 1 ? 1 : cps;
-            const int ncb = cout / nb;
-            int gx = sms * cps / ncb;
-            gx = gx < 1 ? 1 : (gx > tiles ? tiles : gx);
-            OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_umma_res, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            k_conv3x3_umma_res<<<dim3((unsigned)gx, (unsigned)ncb), 256, smem, (cudaStream_t)stream>>>(a, maps, nb,
-                                                                                                     tiles);
-            return launch_status();
-        }
-        const dim3 grid((unsigned)tiles, (unsigned)(cout / nb));
-        const int nst = conv_stages(nb);
-        const int smem = umma_smem_bytes(nb, nst);
-        auto kern = nst == 2 ? k_conv3x3_umma<2> : nst == 3 ? k_conv3x3_umma<3> : k_conv3x3_umma<4>;
-        OTF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        kern<<<grid, 128, smem, (cudaStream_t)stream>>>(a, maps, nb);
-        return launch_status();
+        return conv_umma_launch(a, maps, nb, nk, tiles, (cudaStream_t)stream);
     }
     const int tiles = ((W + TW - 1) / TW) * ((H + TH - 1) / TH) * N;
     k_conv3x3<<<dim3((unsigned)tiles, (unsigned)(cout / BN)), 128, 0, (cudaStream_t)stream>>>(a);
+    return launch_status();
+}
+
+int otf_unet_conv3x3(const void *src0, int c0, const void *src1, int c1, int up1, const void *w,
+                     const float *bias, int relu, void *dst0, const void *mask0, void *dst1,
+                     const void *mask1, int split, int cout, int N, int H, int W, void *stream)
+{
+    return otf_unet_conv3x3_packed(src0, c0, src1, c1, up1, w, nullptr, bias, relu, dst0, mask0, dst1, mask1,
+                                   split, cout, N, H, W, stream);
+}
+
+int otf_unet_pack_weights_tc(const void *w, int cout, int cin, void *wp, void *stream)
+{
+    OTF_CHECK(cin % 16 == 0 && cout > 0, 1, "pack_weights_tc: cin must be a multiple of 16");
+    const int64_t units = (int64_t)(cin / 8) * 9 * cout;
+    const int nbk = (int)std::min<int64_t>((units + 255) / 256, 4 * 148);
+    k_pack_w_umma<<<nbk, 256, 0, (cudaStream_t)stream>>>((const bf16 *)w, (bf16 *)wp, cout, cin);
     return launch_status();
 }
 

@@ -8,10 +8,11 @@
 //
 // Warp roles, each stage a full / empty mbarrier pair:
 //   warps 0, 2, 3 (producers): per 16-channel chunk, warp 0 loads the chunk's
-//     weights of every tap ([tap][cout][8 ch] per 8-channel plane: one 3D TMA
-//     load per plane) and the input halo (34 x 10 pixels x 8 channels per
-//     plane: one 4D TMA load per plane; the tensor map's zero fill supplies
-//     the image border); a chunk of the upsampled second input is gathered
+//     weights of every tap ([tap][cout][8 ch] per 8-channel plane: 18 bulk
+//     copies from the packed weights, or two tiled loads, load_chunk_weights)
+//     and the input halo
+//     (34 x 10 pixels x 8 channels per plane: one 4D TMA load per plane; the
+//     tensor map's zero fill supplies the image border); a chunk of the upsampled second input is gathered
 //     by the three warps with cp.async instead (nearest upsampling on load),
 //     then made visible to the tensor cores (fence.proxy.async); each warp
 //     arrives on the stage's full barrier;
@@ -129,12 +130,46 @@ constexpr int HPIX2 = HWU * HH2;                           // 340 halo pixels
 constexpr int PLANE2 = ((HPIX2 * 16 + 127) / 128) * 128;   // one 8-channel halo plane, 128-byte aligned
 }  // namespace umma
 
-// Tensor maps of one convolution: weights [9][cout][cin] as (cin, cout, 9),
-// box (8, N, 9); the inputs [N][H][W][c] as (c, W, H, N), box (8, 10, 34, 1)
-// (x1: the second input at full resolution; unused when it is upsampled).
+// Tensor maps of one convolution: the inputs [N][H][W][c] as (c, W, H, N),
+// box (8, 10, 34, 1) (x1: the second input at full resolution; unused when
+// it is upsampled).
 struct ConvMaps {
-    CUtensorMap w, x0, x1;
+    CUtensorMap w, x0, x1;  // w: weights (cin, cout, 9), box (8, N, 9); used when no packed copy is given
 };
+
+// The weights of chunk kc for output channels [co0, co0 + N) into
+// [plane][tap][co][8 ch] at dst (2 x 9 x N x 16 bytes, completion on bar).
+// With the packed layout a.wp [cin / 8][9][cout][8] (k_pack_w_umma): 18
+// contiguous runs of N x 16 bytes, one bulk copy each, whole sectors;
+// otherwise two tiled loads of the [9][cout][cin] weights with an 8-channel
+// box, 16 bytes per row.
+__device__ __forceinline__ void load_chunk_weights(unsigned char *dst, const ConvArgs &a, const ConvMaps &maps,
+                                                   int kc, int co0, int N, uint64_t *bar)
+{
+    if (a.wp) {
+        for (int pt = 0; pt < 18; pt++) {  // plane * 9 + tap
+            const int plane = pt / 9, tap = pt - 9 * plane;
+            const bf16 *src = a.wp + ((int64_t)((kc * 2 + plane) * 9 + tap) * a.cout + co0) * 8;
+            otf::bulk_load(dst + pt * N * 16, src, (uint32_t)(N * 16), bar);
+        }
+    } else {
+        for (int h = 0; h < 2; h++)
+            otf::tma_load_3d(dst + h * 9 * N * 16, &maps.w, kc * KC + 8 * h, co0, 0, bar);
+    }
+}
+
+// w [9][cout][cin] -> wp [cin / 8][9][cout][8], 16 bytes per thread and step.
+__global__ void k_pack_w_umma(const bf16 *__restrict__ w, bf16 *__restrict__ wp, int cout, int cin)
+{
+    const int64_t n = (int64_t)(cin / 8) * 9 * cout;
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+        const int co = (int)(u % cout);
+        const int64_t r = u / cout;
+        const int tap = (int)(r % 9), cp = (int)(r / 9);
+        reinterpret_cast<uint4 *>(wp)[u] =
+            *reinterpret_cast<const uint4 *>(w + ((int64_t)tap * cout + co) * cin + cp * 8);
+    }
+}
 
 // dynamic shared memory: NST stages of (two halo planes, two weight planes),
 // then 2 NST + 1 barriers, the tensor-memory slot and the failure flag
@@ -283,7 +318,8 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ Co
         // cp.async gather of an upsampled chunk; each arrives once per chunk
         const int pi = warp == 0 ? 0 : warp - 1;
         if (warp == 0 && lane == 0) {
-            otf::tma_prefetch_desc(&maps.w);
+            if (!a.wp)
+                otf::tma_prefetch_desc(&maps.w);
             otf::tma_prefetch_desc(&maps.x0);
             if (a.c1 && !a.up1)
                 otf::tma_prefetch_desc(&maps.x1);
@@ -308,8 +344,7 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ Co
             const bool gather = from1 && a.up1;
             if (warp == 0 && lane == 0) {
                 otf::mbar_expect_tx(&full[s], wbytes + (gather ? 0u : abytes));
-                for (int h = 0; h < 2; h++)
-                    otf::tma_load_3d(st + 2 * umma::PLANE2 + h * 9 * N * 16, &maps.w, ch + 8 * h, co0, 0, &full[s]);
+                load_chunk_weights(st + 2 * umma::PLANE2, a, maps, kc, co0, N, &full[s]);
                 if (!gather) {
                     const CUtensorMap *mx = from1 ? &maps.x1 : &maps.x0;
                     const int c = from1 ? ch - a.c0 : ch;
@@ -373,36 +408,39 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ Co
     }
 }
 
-// Persistent form for the small layers (the CTA's output channels N <= 128
-// and all of its weights within kResWeightBytes): the weights of every chunk
-// and tap stay in shared memory for the CTA's life (one TMA load per chunk
-// and plane at the start, then only halo tiles stream); the CTA walks
-// 256-pixel tiles blockIdx.x, + gridDim.x, ...; two accumulator buffers (2 x
-// 2N tensor-memory columns) let the epilogue of one tile overlap the MMAs of
-// the next. Warps: 0 producer (halo TMA loads; with warps 6 and 7 the
-// cp.async gather of an upsampled chunk), 1 the MMA issuer (one thread),
-// 2-5 the epilogue (TMEM lane quarters 2, 3, 0, 1). Per halo stage a full
-// (three producer warps) / empty (MMA commit) barrier pair; per accumulator
-// buffer a full (MMA commit) / empty (four epilogue warps) pair. Bounded
-// waits as the kernel above; a failed wait sets the error flag, the role
-// stops, and teardown waits (bounded) for the MMAs and copies issued.
+// Persistent forms for the layers with at most 128 output channels per CTA:
+// the CTA walks 256-pixel tiles blockIdx.x, + gridDim.x, ...; two
+// accumulator buffers (2 x 2N tensor-memory columns) let the epilogue of one
+// tile overlap the MMAs of the next. RES (the small layers, all of the CTA's
+// weights within kResWeightBytes): the weights of every chunk and tap stay in
+// shared memory for the CTA's life (one TMA load per chunk and plane at the
+// start, then only halo tiles stream). Otherwise each stage carries a chunk's
+// halo and its weights, NST stages deep. Warps: 0 producer (TMA loads; with
+// warps 6 and 7 the cp.async gather of an upsampled chunk), 1 the MMA
+// issuer (one thread), 2-5 the epilogue (TMEM lane quarters 2, 3, 0, 1). Per
+// stage a full (three producer warps) / empty (MMA commit) barrier pair; per
+// accumulator buffer a full (MMA commit) / empty (four epilogue warps) pair.
+// Bounded waits as the kernel above; a failed wait sets the error flag, the
+// role stops, and teardown waits (bounded) for the MMAs and copies issued.
 constexpr int kResWeightBytes = 96 * 1024;
 constexpr int kResStages = 4;
 __host__ __device__ constexpr int umma_res_smem_bytes(int n, int nk)
 {
     return nk * 2 * 9 * n * 16 + kResStages * 2 * umma::PLANE2 + 256;
 }
+// streamed weights: NST stages of (two halo planes, two weight planes)
+__host__ __device__ constexpr int umma_pers_smem_bytes(int n, int nst) { return nst * umma_stage_bytes(n) + 256; }
 
-__global__ void __launch_bounds__(256) k_conv3x3_umma_res(const __grid_constant__ ConvArgs a,
+template <bool RES, int NST>
+__global__ void __launch_bounds__(256) k_conv3x3_umma_pers(const __grid_constant__ ConvArgs a,
                                                           const __grid_constant__ ConvMaps maps, int N, int n_tiles)
 {
     extern __shared__ __align__(1024) unsigned char smu[];
-    constexpr int NST = kResStages;
     const int cin = a.c0 + a.c1, nk = cin / KC;
     const int wchunk = 2 * 9 * N * 16;          // bytes of one chunk's weights (two planes)
-    unsigned char *wsm = smu;                   // [chunk][plane][tap][co][8 ch]
-    unsigned char *hsm = smu + nk * wchunk;     // NST halo stages of two planes
-    constexpr int SA = 2 * umma::PLANE2;
+    unsigned char *wsm = smu;                   // RES: [chunk][plane][tap][co][8 ch]
+    unsigned char *hsm = RES ? smu + nk * wchunk : smu;  // NST stages
+    const int SA = 2 * umma::PLANE2 + (RES ? 0 : wchunk);  // a stage: halo planes (+ chunk weights)
     uint64_t *full = reinterpret_cast<uint64_t *>(hsm + NST * SA);
     uint64_t *empty = full + NST;
     uint64_t *acc_full = empty + NST;
@@ -453,14 +491,18 @@ __global__ void __launch_bounds__(256) k_conv3x3_umma_res(const __grid_constant_
         // producers
         const int pi = warp == 0 ? 0 : warp - 5;
         if (warp == 0 && lane == 0) {
-            otf::tma_prefetch_desc(&maps.w);
+            if (!a.wp)
+                otf::tma_prefetch_desc(&maps.w);
             otf::tma_prefetch_desc(&maps.x0);
             if (a.c1 && !a.up1)
                 otf::tma_prefetch_desc(&maps.x1);
-            otf::mbar_arrive_expect_tx(wbar, (uint32_t)(nk * wchunk));
-            for (int kc = 0; kc < nk; kc++)
-                for (int h = 0; h < 2; h++)
-                    otf::tma_load_3d(wsm + kc * wchunk + h * 9 * N * 16, &maps.w, kc * KC + 8 * h, co0, 0, wbar);
+            if (RES) {
+                otf::mbar_arrive_expect_tx(wbar, (uint32_t)(nk * wchunk));
+                for (int kc = 0; kc < nk; kc++)
+                    load_chunk_weights(wsm + kc * wchunk, a, maps, kc, co0, N, wbar);
+            } else {
+                otf::mbar_arrive(wbar);  // nothing resident to wait for
+            }
         }
         const uint32_t abytes = 2u * umma::HPIX2 * 16u;
         int g = 0;
@@ -485,12 +527,16 @@ __global__ void __launch_bounds__(256) k_conv3x3_umma_res(const __grid_constant_
                 const int ch = kc * KC;
                 const bool from1 = ch >= a.c0;
                 const bool gather = from1 && a.up1;
-                if (warp == 0 && lane == 0 && !gather) {
-                    otf::mbar_expect_tx(&full[s], abytes);
-                    const CUtensorMap *mx = from1 ? &maps.x1 : &maps.x0;
-                    const int c = from1 ? ch - a.c0 : ch;
-                    for (int h = 0; h < 2; h++)
-                        otf::tma_load_4d(st + h * umma::PLANE2, mx, c + 8 * h, x0 - 1, y0 - 1, n, &full[s]);
+                if (warp == 0 && lane == 0 && (!gather || !RES)) {
+                    otf::mbar_expect_tx(&full[s], (gather ? 0u : abytes) + (RES ? 0u : (uint32_t)wchunk));
+                    if (!RES)
+                        load_chunk_weights(st + 2 * umma::PLANE2, a, maps, kc, co0, N, &full[s]);
+                    if (!gather) {
+                        const CUtensorMap *mx = from1 ? &maps.x1 : &maps.x0;
+                        const int c = from1 ? ch - a.c0 : ch;
+                        for (int h = 0; h < 2; h++)
+                            otf::tma_load_4d(st + h * umma::PLANE2, mx, c + 8 * h, x0 - 1, y0 - 1, n, &full[s]);
+                    }
                 }
                 if (gather)
                     conv_gather(a, st, ch, n, y0, x0, pi, 3, lane);
@@ -527,7 +573,7 @@ __global__ void __launch_bounds__(256) k_conv3x3_umma_res(const __grid_constant_
                     }
                     umma::fence_after_sync();
                     const uint32_t abase = otf::smem_u32(hsm + s * SA);
-                    const uint32_t bbase = otf::smem_u32(wsm + kc * wchunk);
+                    const uint32_t bbase = RES ? otf::smem_u32(wsm + kc * wchunk) : abase + 2 * umma::PLANE2;
 #pragma unroll
                     for (int tap = 0; tap < 9; tap++) {
                         const int dy = tap / 3, dx = tap - 3 * (tap / 3);

@@ -32,6 +32,8 @@ def _declare(L):
     v, i, f, ll = c_void_p, c_int, c_float, c_longlong
     sig = {
         "otf_unet_conv3x3": [v, i, v, i, i, v, v, i, v, v, v, v, i, i, i, i, i, v],
+        "otf_unet_conv3x3_packed": [v, i, v, i, i, v, v, v, i, v, v, v, v, i, i, i, i, i, v],
+        "otf_unet_pack_weights_tc": [v, i, i, v, v],
         "otf_unet_conv3x3_wgrad": [v, i, v, i, i, v, i, v, i, i, i, i, v],
         "otf_unet_bias_grad": [v, i, ll, v, v],
         "otf_unet_pool2": [v, v, i, i, i, i, v],
@@ -90,9 +92,12 @@ class UNet:
         self.v = torch.zeros_like(self.params)
         self.step_count = 0
         self.wf, self.wb = {}, {}
+        self.wfp, self.wbp = {}, {}  # the same, packed for the tcgen05 kernels' bulk copies
         for name, cin, cout in self.layers:
             self.wf[name] = torch.empty(9 * cout * cin, dtype=torch.bfloat16, device=self.dev)
             self.wb[name] = torch.empty(9 * cout * cin, dtype=torch.bfloat16, device=self.dev)
+            self.wfp[name] = torch.empty(9 * cout * cin, dtype=torch.bfloat16, device=self.dev)
+            self.wbp[name] = torch.empty(9 * cout * cin, dtype=torch.bfloat16, device=self.dev)
         self.sm = torch.cuda.get_device_properties(self.dev).multi_processor_count
         self._bufs = {}
         self.loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
@@ -131,11 +136,14 @@ class UNet:
             raise _lib.OtfwiError("unet kernel failed")
 
     def pack(self):
-        """BF16 forward and input-gradient copies of every conv weight."""
+        """BF16 forward and input-gradient copies of every conv weight, and
+        both regrouped by 8-channel plane for the tcgen05 kernels."""
         st = self._stream()
         for name, cin, cout in self.layers:
             self._ok(self.L.otf_unet_pack_weights(_p(self.weight(name)), cout, cin, _p(self.wf[name]),
                                                   _p(self.wb[name]), st))
+            self._ok(self.L.otf_unet_pack_weights_tc(_p(self.wf[name]), cout, cin, _p(self.wfp[name]), st))
+            self._ok(self.L.otf_unet_pack_weights_tc(_p(self.wb[name]), cin, cout, _p(self.wbp[name]), st))
 
     def state(self):
         return self.params.detach().cpu().numpy().copy()
@@ -197,17 +205,17 @@ class UNet:
         c0 = src0.shape[-1]
         c1 = 0 if src1 is None else src1.shape[-1]
         assert c0 + c1 == cin
-        self._ok(self._timed("fwd", name, 18.0 * cin * cout * N * H * W, lambda: self.L.otf_unet_conv3x3(
-            _p(src0), c0, _p(src1), c1, up1, _p(self.wf[name]), _p(self.bias(name)), relu, _p(dst), None, None,
-            None, cout, cout, N, H, W, self._stream())))
+        self._ok(self._timed("fwd", name, 18.0 * cin * cout * N * H * W, lambda: self.L.otf_unet_conv3x3_packed(
+            _p(src0), c0, _p(src1), c1, up1, _p(self.wf[name]), _p(self.wfp[name]), _p(self.bias(name)), relu,
+            _p(dst), None, None, None, cout, cout, N, H, W, self._stream())))
 
     def _dgrad(self, name, dz, dst0, mask0, N, H, W, dst1=None, split=None):
         """input gradient of conv `name` from its pre-activation gradient dz."""
         _, cin, cout = next(l for l in self.layers if l[0] == name)
         split = cin if split is None else split
-        self._ok(self._timed("dgrad", name, 18.0 * cin * cout * N * H * W, lambda: self.L.otf_unet_conv3x3(
-            _p(dz), cout, None, 0, 0, _p(self.wb[name]), None, 0, _p(dst0), _p(mask0), _p(dst1), None, split, cin,
-            N, H, W, self._stream())))
+        self._ok(self._timed("dgrad", name, 18.0 * cin * cout * N * H * W, lambda: self.L.otf_unet_conv3x3_packed(
+            _p(dz), cout, None, 0, 0, _p(self.wb[name]), _p(self.wbp[name]), None, 0, _p(dst0), _p(mask0),
+            _p(dst1), None, split, cin, N, H, W, self._stream())))
 
     def _wgrad(self, name, src0, dz, N, H, W, src1=None, up1=0):
         _, cin, cout = next(l for l in self.layers if l[0] == name)
@@ -332,8 +340,9 @@ class UNet:
 
 
 def _bench_conv(a):
-    """One forward convolution (bias + ReLU) of the given shape, launched
-    `iters` times after 3 warm-up launches, timed with CUDA events."""
+    """One forward convolution (bias + ReLU) of the given shape, with the
+    weights packed as the network passes them, launched `iters` times after 3
+    warm-up launches, timed with CUDA events."""
     import json
 
     import torch
@@ -347,10 +356,13 @@ def _bench_conv(a):
     b = torch.zeros(cout, device="cuda")
     y = torch.empty(N, H, W, cout, dtype=torch.bfloat16, device="cuda")
     st = c_void_p(torch.cuda.current_stream().cuda_stream)
+    wp = torch.empty_like(w)  # packed once, as the network packs after each update
+    if L.otf_unet_pack_weights_tc(_p(w), cout, cin, _p(wp), st) != 0:
+        _lib.check(L)
 
     def launch():
-        if L.otf_unet_conv3x3(_p(x), cin, None, 0, 0, _p(w), _p(b), 1, _p(y), None, None, None, cout, cout,
-                              N, H, W, st) != 0:
+        if L.otf_unet_conv3x3_packed(_p(x), cin, None, 0, 0, _p(w), _p(wp), _p(b), 1, _p(y), None, None, None,
+                                     cout, cout, N, H, W, st) != 0:
             _lib.check(L)
 
     for _ in range(3):

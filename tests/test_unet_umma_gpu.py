@@ -11,7 +11,9 @@ input gradient's form). Convolution outputs are BF16: relative L2 <= 1e-2
 against the oracle, as the other U-Net tests; the two kernels sum the same
 products in different orders, so they agree to a few BF16 roundings
 (relative L2 <= 5e-3). Weight gradients are FP32 sums: relative L2 <= 1e-4.
-The kernels' bounded waits must all have completed (device status 0)."""
+With the weights packed for bulk copies (otf_unet_conv3x3_packed) the
+result is bit-identical. The kernels' bounded waits must all have completed
+(device status 0)."""
 import numpy as np
 import pytest
 
@@ -80,6 +82,16 @@ def test_umma_conv_vs_oracle_and_legacy(lib, case):
         torch.cuda.synchronize()
         outs[umma] = (_np(D0), _np(D1)[..., :cout - split])
     L.otf_unet_set_umma(1)
+    # the same convolution with the weights packed for bulk copies: the same
+    # shared-memory layout, so the same result bit for bit
+    Wp = torch.empty_like(Wt)
+    assert L.otf_unet_pack_weights_tc(_p(Wt), cout, c0 + c1, _p(Wp), st) == 0
+    P0 = torch.full((N, H, W, split), float("nan"), dtype=torch.bfloat16, device="cuda")
+    P1 = torch.full((N, H, W, max(cout - split, 1)), float("nan"), dtype=torch.bfloat16, device="cuda")
+    assert L.otf_unet_conv3x3_packed(_p(X0), c0, _p(X1), c1, up1, _p(Wt), _p(Wp), _p(B), relu, _p(P0), _p(M0),
+                                     _p(P1) if split < cout else None, None, split, cout, N, H, W, st) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(_np(P0), outs[1][0]) and np.array_equal(_np(P1)[..., :cout - split], outs[1][1])
     assert L.otf_unet_status() == 0
     net = uo.Net(np.zeros(uo.n_params(4), np.float32), 4)
     xin = _np(X0)
