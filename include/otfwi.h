@@ -273,9 +273,10 @@ int otf_unet_pack_weights_tc(const void *w, int cout, int cin, void *wp, void *s
  * gradient dz [N][H][W][cout] of that convolution's inputs. */
 int otf_unet_conv3x3_wgrad(const void *src0, int c0, const void *src1, int c1, int up1, const void *dz,
                            int cout, float *dw, int N, int H, int W, int sm_count, void *stream);
-/* Tensor-core path of the two functions above: 1 = tcgen05 / UMMA kernels
- * with tensor-memory accumulators (default; the weight gradient of layers
- * with cin x cout below 128 x 128 keeps the mma.sync kernel, measured faster
+/* Tensor-core path of the functions above: 1 = tcgen05 / UMMA kernels with
+ * tensor-memory accumulators (default; the weight gradients of 16-input-
+ * channel layers, of 32 -> 64 channels and of a concatenation with an
+ * upsampled input into 32 channels keep the mma.sync kernel, measured faster
  * there), 2 = tcgen05 for every shape, 0 = the warp-level mma.sync kernels;
  * returns the previous setting (process-wide). */
 int otf_unet_set_umma(int on);

@@ -766,10 +766,9 @@ int otf_unet_pack_weights_tc(const void *w, int cout, int cin, void *wp, void *s
 }
 
 /* Tensor-core path of the 3x3 convolution and its weight gradient: 1 =
- * tcgen05 (default; the weight gradient of layers with cin x cout below
- * 128 x 128 keeps the mma.sync kernel, which is faster there), 2 = tcgen05
- * for every shape, 0 = the warp-level mma.sync kernels; returns the previous
- * setting. */
+ * tcgen05 (default; the weight gradients of three small layer shapes keep
+ * the mma.sync kernel, which is faster there), 2 = tcgen05 for every shape,
+ * 0 = the warp-level mma.sync kernels; returns the previous setting. */
 int otf_unet_set_umma(int on)
 {
     const int prev = g_use_umma;
@@ -809,34 +808,57 @@ int otf_unet_conv3x3_wgrad(const void *src0, int c0, const void *src1, int c1, i
     a.N = N;
     a.H = H;
     a.W = W;
-    // The tcgen05 weight gradient computes 128 output channels per CTA (rows
-    // beyond cout are zeros): measured per layer of the 16 x 256^2 network it
-    // beats the mma.sync kernel where cin x cout >= 128 x 128 (1.1-1.8x) and
-    // loses below (0.6-0.9x), so smaller layers keep the mma.sync kernel.
-    if (use_umma() && (g_use_umma == 2 || (int64_t)(c0 + c1) * cout >= 128 * 128)) {
+    // The tcgen05 weight gradient computes 128 output-channel rows per CTA
+    // (rows beyond cout are zeros) and gathers the upsampled input three times
+    // (once per dx window): measured per layer of the 16 x 256^2 network it
+    // beats the mma.sync kernel on every layer (1.1-1.6x) but three, which
+    // keep the mma.sync kernel: 16 input channels (84 against 100 TFLOP/s),
+    // 32 -> 64 channels (104 / 112) and 32 + 64 upsampled -> 32 (79 / 129).
+    const int cin_all = c0 + c1;
+    const bool tc = cin_all >= 32 && !(cout < 128 && cin_all < 64 && cout > cin_all) && !(up1 && c1 > 0 && cout < 64);
+    if (use_umma() && (g_use_umma == 2 || tc)) {
         // tensor-core path: 128 output channels x 32 (or 16) input channels x
         // 9 taps per CTA, the pixels split into slab ranges so that about one
-        // CTA per SM (two with 16 input channels) runs
+        // CTA per SM runs
         const int cin = c0 + c1;
         const int nw = cin % 32 == 0 ? 32 : 16;
         const int n_slabs = ((W + umma::TWU - 1) / umma::TWU) * ((H + umma::THU - 1) / umma::THU) * N;
         const int gy = (cout + 127) / 128, gz = cin / nw;
-        const int target = (sm_count > 0 ? sm_count : 148) * (nw == 32 ? 1 : 2);
+        const int target = sm_count > 0 ? sm_count : 148;  // one CTA per SM (140-181 KB of stages)
         int gx = target / (gy * gz);
         gx = gx < 1 ? 1 : (gx > n_slabs ? n_slabs : gx);
         const int spc = (n_slabs + gx - 1) / gx;
         gx = (n_slabs + spc - 1) / spc;
         const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)gz);
+        WgradMaps maps;
+        std::memset(&maps, 0, sizeof(maps));
+        {
+            const cuuint64_t dims[4] = {(cuuint64_t)cout, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+            const cuuint64_t str[3] = {(cuuint64_t)cout * 2, (cuuint64_t)W * cout * 2, (cuuint64_t)H * W * cout * 2};
+            const cuuint32_t box[4] = {8, (cuuint32_t)umma::TWU, (cuuint32_t)umma::THU, 1};
+            if (encode_bf16_map(&maps.dz, dz, 4, dims, str, box))
+                return -1;
+        }
+        for (int i = 0; i < 2; i++) {
+            const int c = i ? c1 : c0;
+            if (c == 0 || (i == 1 && up1))
+                continue;
+            const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+            const cuuint64_t str[3] = {(cuuint64_t)c * 2, (cuuint64_t)W * c * 2, (cuuint64_t)H * W * c * 2};
+            const cuuint32_t box[4] = {8, (cuuint32_t)umma::TWU, (cuuint32_t)umma::THU + 2, 1};
+            if (encode_bf16_map(i ? &maps.x1 : &maps.x0, i ? src1 : src0, 4, dims, str, box))
+                return -1;
+        }
         if (nw == 32) {
             const int smem = umma_wg_smem_bytes(32, 3);
             OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_wgrad_umma<32, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           smem));
-            k_conv3x3_wgrad_umma<32, 3><<<grid, 128, smem, (cudaStream_t)stream>>>(a, spc);
+            k_conv3x3_wgrad_umma<32, 3><<<grid, 128, smem, (cudaStream_t)stream>>>(a, maps, spc);
         } else {
             const int smem = umma_wg_smem_bytes(16, 3);
             OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_wgrad_umma<16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           smem));
-            k_conv3x3_wgrad_umma<16, 3><<<grid, 128, smem, (cudaStream_t)stream>>>(a, spc);
+            k_conv3x3_wgrad_umma<16, 3><<<grid, 128, smem, (cudaStream_t)stream>>>(a, maps, spc);
         }
         return launch_status();
     }

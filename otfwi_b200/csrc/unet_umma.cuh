@@ -626,44 +626,67 @@ __global__ void __launch_bounds__(256) k_conv3x3_umma_pers(const __grid_constant
     }
 }
 
-// Weight gradient on the tcgen05 tensor cores: for each tap,
+// Weight gradient on the tcgen05 tensor cores:
 //
-//   D_tap[co][ci] += sum over pixels p of dz[p][co] * x[p + tap][ci],
+//   dW[dy * 3 + dx][co][ci] += sum over pixels p of dz[p][co] * x[p + (dy - 1, dx - 1)][ci],
 //
-// an implicit GEMM with M = 128 output channels (rows beyond cout staged as
-// zeros), N = 32 input channels (16 when the layer has 16), K = pixels, 16
-// (two tile rows) per MMA; the 9 taps' accumulators sit side by side in
-// tensor memory (9 x N columns). Both operands are MN-major (channels
-// contiguous, as the activations are stored): per 128-pixel slab (8 x 16) the
-// CTA stages dz as [co / 8][pixel][8 co] and the input halo as [ci / 8][halo
-// pixel][8 ci], the no-swizzle MN-major canonical UMMA layout (a core matrix
-// is 8 channels x 8 pixels, 128 contiguous bytes). For tap (dy, dx) and K
-// step s the B operand starts at halo pixel (2s + dy) * 10 + dx: eight
-// pixels of one tile row are eight consecutive halo pixels, the next tile row
-// is one halo row (160 bytes) further. A CTA walks a range of slabs, then adds
-// its 9 x 128 x N partial sums to dw with FP32 atomics (the mma.sync kernel's
-// reduction). Bounded waits as the forward kernel.
-__host__ __device__ constexpr int umma_wg_stage_bytes(int nw) { return 128 * 256 + (nw / 8) * umma::PLANE_A; }
-__host__ __device__ constexpr int umma_wg_smem_bytes(int nw, int nst) { return nst * umma_wg_stage_bytes(nw) + 128; }
+// an implicit GEMM per CTA with M = 128 output channels (rows beyond cout are
+// the zero fill of the dz tensor map), N = the three dx taps x NW input
+// channels (96 or 48), K = pixels, 16 (two rows of an 8 x 16 slab) per MMA;
+// the three dy taps are three accumulators (3 N tensor-memory columns). Both
+// operands are MN-major (channels contiguous, as stored): a core matrix is 8
+// channels x 8 pixels, 128 contiguous bytes. Per slab a stage holds dz as
+// [co / 8][128 pixels][8 co] (16 TMA boxes of 8 channels x 8 x 16 pixels) and,
+// for each dx, the input's 8-column window shifted by dx over the slab's 18
+// halo rows as [dx][ci / 8][18 x 8 pixels][8 ci] (3 NW / 8 boxes of 8 x 8 x
+// 18; an upsampled input gathered by cp.async instead). The B operand of dy
+// and K step s then starts at halo row 2 s + dy of every (dx, ci group)
+// window: K groups 128 bytes apart, N groups one window (2304 bytes) apart;
+// 24 MMAs per slab instead of 72 with one tap per accumulator, and a
+// third of the shared-memory operand reads per multiply-add. Warp roles as
+// the forward kernel: warps 0, 2, 3 stage (lane 0 of warp 0 the TMA loads,
+// the three warps the gather), one thread of warp 1 issues the MMAs, then
+// the four warps add the CTA's 9 x 128 x NW partial sums to dw with FP32
+// atomics. Bounded waits as the forward kernel.
+namespace umma {
+constexpr int WG_A = 16 * 128 * 16;   // dz of a slab: 16 groups of 8 channels x 128 pixels x 16 bytes
+constexpr int WG_WIN = 18 * 8 * 16;   // one (dx, channel group) window: 18 halo rows x 8 pixels x 16 bytes
+}  // namespace umma
+__host__ __device__ constexpr int umma_wg_stage_bytes(int nw) { return umma::WG_A + 3 * (nw / 8) * umma::WG_WIN; }
+__host__ __device__ constexpr int umma_wg_smem_bytes(int nw, int nst) { return nst * umma_wg_stage_bytes(nw) + 256; }
 
 __host__ __device__ constexpr uint32_t instr_desc_bf16_mn(int n)
 {
     return umma::instr_desc_bf16(n) | (1u << 15) | (1u << 16);  // A and B MN-major
 }
 
+// Tensor maps of one weight gradient: dz (cout, W, H, N), box (8, 8, 16, 1);
+// the inputs (c, W, H, N), box (8, 8, 18, 1) (x1 at full resolution; unused
+// when upsampled).
+struct WgradMaps {
+    CUtensorMap dz, x0, x1;
+};
+
 template <int NW, int NST>
-__global__ void __launch_bounds__(128) k_conv3x3_wgrad_umma(WgradArgs a, int slabs_per_cta)
+__global__ void __launch_bounds__(128) k_conv3x3_wgrad_umma(const __grid_constant__ WgradArgs a,
+                                                            const __grid_constant__ WgradMaps maps, int slabs_per_cta)
 {
     extern __shared__ __align__(1024) unsigned char smu[];
     constexpr int SB = umma_wg_stage_bytes(NW);
-    constexpr uint32_t NCOLS = 9 * NW <= 256 ? 256u : 512u;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smu + NST * SB);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + NST + 1);
+    constexpr int NB = 3 * NW;                       // N of one MMA: 3 dx taps x NW channels
+    constexpr uint32_t NCOLS = 3 * NB <= 256 ? 256u : 512u;
+    constexpr int NG = NW / 8;                       // input channel groups
+    uint64_t *full = reinterpret_cast<uint64_t *>(smu + NST * SB);
+    uint64_t *empty = full + NST;
+    uint64_t *done = empty + NST;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
+    int *fail = reinterpret_cast<int *>(tslot + 1);
     const int co0 = blockIdx.y * 128, ci0 = blockIdx.z * NW;
     const int cin = a.c0 + a.c1;
     const int tiles_x = (a.W + umma::TWU - 1) / umma::TWU, tiles_y = (a.H + umma::THU - 1) / umma::THU;
     const int n_slabs = tiles_x * tiles_y * a.N;
     const int s_begin = blockIdx.x * slabs_per_cta, s_end = min(n_slabs, s_begin + slabs_per_cta);
+    const int nsl = s_end > s_begin ? s_end - s_begin : 0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     ConvArgs ca{};
     ca.src0 = a.src0;
@@ -676,8 +699,11 @@ __global__ void __launch_bounds__(128) k_conv3x3_wgrad_umma(WgradArgs a, int sla
     ca.W = a.W;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s <= NST; s++)
-            otf::mbar_init(&bar[s], 1);
+        for (int i = 0; i < NST; i++)
+            otf::mbar_init(&full[i], 3);  // one arrival per producer warp
+        for (int i = NST; i < 2 * NST + 1; i++)
+            otf::mbar_init(&full[i], 1);  // empty barriers and `done`: one commit each
+        *fail = 0;
         otf::fence_barrier_init();
     }
     if (warp == 0)
@@ -686,93 +712,133 @@ __global__ void __launch_bounds__(128) k_conv3x3_wgrad_umma(WgradArgs a, int sla
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t idesc = instr_desc_bf16_mn(NW);
 
-    auto load = [&](int slab, unsigned char *st) {
-        int b = slab;
-        const int n = b / (tiles_x * tiles_y);
-        b -= n * tiles_x * tiles_y;
-        const int ty = b / tiles_x, tx = b - ty * tiles_x;
-        const int y0 = ty * umma::THU, x0 = tx * umma::TWU;
-        uint32_t *sd = reinterpret_cast<uint32_t *>(st);
-        // dz: 128 pixels x 128 output channels, 8 channels per copy
-        for (int i = threadIdx.x; i < 128 * 16; i += 128) {
-            const int g = i >> 7, px = i & 127;  // channel group, pixel (oy * 8 + ox)
-            const int y = y0 + (px >> 3), x = x0 + (px & 7), co = co0 + g * 8;
-            const bool ok = y < a.H && x < a.W && co < a.cout;
-            const void *src = ok ? (const void *)(a.dz + (((int64_t)n * a.H + y) * a.W + x) * a.cout + co)
-                                 : (const void *)a.dz;
-            cp_async16(sd + (g * 128 + px) * 4, src, ok ? 16 : 0);
+    if (warp != 1) {
+        // producers: warp 0 issues the TMA loads; warps 0, 2 and 3 share the
+        // gather of the upsampled channel groups; each arrives once per slab
+        const int pi = warp == 0 ? 0 : warp - 1;
+        if (warp == 0 && lane == 0) {
+            otf::tma_prefetch_desc(&maps.dz);
+            otf::tma_prefetch_desc(&maps.x0);
+            if (a.c1 && !a.up1)
+                otf::tma_prefetch_desc(&maps.x1);
         }
-        uint32_t *sx = reinterpret_cast<uint32_t *>(st + 128 * 256);
-        for (int i = threadIdx.x; i < umma::HPIX * (NW / 8); i += 128) {
-            const int g = i / umma::HPIX, px = i - g * umma::HPIX;
-            const int hy = px / umma::HWU, hx = px - hy * umma::HWU;
-            const int gy = y0 + hy - 1, gx = x0 + hx - 1;
-            const bool ok = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
-            const void *src = ok ? (const void *)in_ptr(ca, n, gy, gx, ci0 + g * 8) : (const void *)a.dz;
-            cp_async16(sx + (g * umma::PLANE_A + px * 16) / 4, src, ok ? 16 : 0);
-        }
-    };
-
-    bool ok = true;
-    const int nsl = s_end - s_begin;
-    if (nsl > 0) {
-        load(s_begin, smu);
-        cp_commit();
-    }
-    for (int k = 0; k < nsl; k++) {
-        const int s = k % NST;
-        if (k + 1 < nsl) {
-            const int s1 = (k + 1) % NST;
-            if (k + 1 >= NST && ok)
-                ok = otf::mbar_wait(&bar[s1], (uint32_t)(((k + 1) / NST - 1) & 1), &g_unet_err);
-            load(s_begin + k + 1, smu + s1 * SB);
-        }
-        cp_commit();
-        cp_wait<1>();
-        umma::fence_proxy_async();
-        __syncthreads();
-        if (threadIdx.x == 0 && ok) {
-            umma::fence_after_sync();
-            const uint32_t abase = otf::smem_u32(smu + s * SB);
-            const uint32_t bbase = abase + 128 * 256;
-#pragma unroll 1
-            for (int tap = 0; tap < 9; tap++) {
-                const int dy = tap / 3, dx = tap - 3 * (tap / 3);
-#pragma unroll
-                for (int ks = 0; ks < 8; ks++) {
-                    // A: channel groups 2048 bytes apart, K groups (tile rows) 128 bytes apart
-                    const uint64_t ad = umma::smem_desc(abase + ks * 256, 128, 128 * 16);
-                    // B: channel groups one plane apart, K groups (tile rows) one halo row apart
-                    const uint64_t bd = umma::smem_desc(bbase + ((2 * ks + dy) * umma::HWU + dx) * 16,
-                                                        umma::HWU * 16, umma::PLANE_A);
-                    umma::mma_bf16(tmem + (uint32_t)(tap * NW), ad, bd, idesc, k > 0 || ks > 0);
+        int issued = 0;
+        for (int k = 0; k < nsl; k++) {
+            const int s = k % NST;
+            if (k >= NST) {
+                int okw = 1;
+                if (lane == 0)
+                    okw = otf::mbar_wait(&empty[s], (uint32_t)((k / NST - 1) & 1), &g_unet_err) ? 1 : 0;
+                if (!__shfl_sync(0xffffffffu, okw, 0)) {
+                    if (lane == 0)
+                        *fail = 1;
+                    break;
                 }
             }
-            umma::mma_commit(&bar[s]);
+            int b = s_begin + k;
+            const int n = b / (tiles_x * tiles_y);
+            b -= n * tiles_x * tiles_y;
+            const int ty = b / tiles_x, tx = b - ty * tiles_x;
+            const int y0 = ty * umma::THU, x0 = tx * umma::TWU;
+            unsigned char *st = smu + s * SB;
+            unsigned char *sx = st + umma::WG_A;
+            if (warp == 0 && lane == 0) {
+                uint32_t bytes = umma::WG_A;
+                for (int g = 0; g < NG; g++)
+                    if (!(a.up1 && ci0 + 8 * g >= a.c0))
+                        bytes += 3u * umma::WG_WIN;
+                otf::mbar_expect_tx(&full[s], bytes);
+                for (int g = 0; g < 16; g++)
+                    otf::tma_load_4d(st + g * 128 * 16, &maps.dz, co0 + 8 * g, x0, y0, n, &full[s]);
+                for (int g = 0; g < NG; g++) {
+                    const int c = ci0 + 8 * g;
+                    if (a.up1 && c >= a.c0)
+                        continue;
+                    const CUtensorMap *mx = c < a.c0 ? &maps.x0 : &maps.x1;
+                    const int cc = c < a.c0 ? c : c - a.c0;
+                    for (int dx = 0; dx < 3; dx++)
+                        otf::tma_load_4d(sx + (dx * NG + g) * umma::WG_WIN, mx, cc, x0 - 1 + dx, y0 - 1, n,
+                                         &full[s]);
+                }
+            }
+            if (a.up1 && ci0 + NW > a.c0) {
+                // channel groups of the upsampled second input: gathered
+                for (int i = pi * 32 + lane; i < 3 * NG * 144; i += 96) {
+                    const int win = i / 144, px = i - win * 144;
+                    const int dx = win / NG, g = win - dx * NG;
+                    const int c = ci0 + 8 * g;
+                    if (c < a.c0)
+                        continue;
+                    const int gy = y0 - 1 + px / 8, gx = x0 - 1 + dx + (px & 7);
+                    const bool in = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
+                    const void *src = in ? (const void *)in_ptr(ca, n, gy, gx, c) : (const void *)a.dz;
+                    cp_async16(reinterpret_cast<uint32_t *>(sx + win * umma::WG_WIN + px * 16), src, in ? 16 : 0);
+                }
+                cp_commit();
+                cp_wait<0>();
+                umma::fence_proxy_async();
+            }
+            __syncwarp();
+            if (lane == 0)
+                otf::mbar_arrive(&full[s]);
+            issued = k + 1;
         }
-        __syncthreads();
+        if (warp == 0 && lane == 0)
+            for (int k = issued > NST ? issued - NST : 0; k < issued; k++)
+                otf::mbar_wait(&full[k % NST], (uint32_t)((k / NST) & 1), &g_unet_err);
+        __syncwarp();
+    } else {
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc_bf16_mn(NB);
+            for (int k = 0; k < nsl; k++) {
+                const int s = k % NST;
+                if (!otf::mbar_wait(&full[s], (uint32_t)((k / NST) & 1), &g_unet_err)) {
+                    *fail = 1;
+                    break;
+                }
+                umma::fence_after_sync();
+                const uint32_t abase = otf::smem_u32(smu + s * SB);
+                const uint32_t bbase = abase + umma::WG_A;
+#pragma unroll
+                for (int dy = 0; dy < 3; dy++) {
+#pragma unroll
+                    for (int ks = 0; ks < 8; ks++) {
+                        // A: channel groups 2048 bytes apart, K groups (tile rows) 128 bytes apart
+                        const uint64_t ad = umma::smem_desc(abase + ks * 256, 128, 128 * 16);
+                        // B: K groups (halo rows) 128 bytes apart, (dx, channel group) windows one window apart
+                        const uint64_t bd = umma::smem_desc(bbase + (2 * ks + dy) * 128, 128, umma::WG_WIN);
+                        umma::mma_bf16(tmem + (uint32_t)(dy * NB), ad, bd, idesc, k > 0 || ks > 0);
+                    }
+                }
+                umma::mma_commit(&empty[s]);
+            }
+            umma::mma_commit(done);
+        }
+        __syncwarp();
     }
-    if (threadIdx.x == 0)
-        umma::mma_commit(&bar[NST]);
-    const bool done = otf::mbar_wait(&bar[NST], 0, &g_unet_err);
-    ok = ok && done;
+    __syncthreads();
+    const bool ok = otf::mbar_wait(done, 0, &g_unet_err) && *fail == 0;
     umma::fence_after_sync();
 
     if (ok && nsl > 0) {
         const int co = co0 + warp * 32 + lane;  // TMEM lane = output channel row
-        for (int tap = 0; tap < 9; tap++) {
-            for (int c = 0; c < NW; c += 16) {
-                // 32 columns from tap * NW + c (inside the allocation); the
-                // first 16 are this (tap, c .. c+15)
-                float v[32];
-                umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(tap * NW + c), v);
-                if (co < a.cout) {
-                    float *d = a.dw + ((int64_t)tap * a.cout + co) * cin + ci0 + c;
+#pragma unroll 1
+        for (int dy = 0; dy < 3; dy++) {
+#pragma unroll 1
+            for (int dx = 0; dx < 3; dx++) {
+#pragma unroll 1
+                for (int c = 0; c < NW; c += 16) {
+                    // 32 columns from (dy, dx, c) (inside the allocation); the
+                    // first 16 are channels c .. c+15 of this tap
+                    float v[32];
+                    umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(dy * NB + dx * NW + c), v);
+                    if (co < a.cout) {
+                        float *d = a.dw + ((int64_t)(dy * 3 + dx) * a.cout + co) * cin + ci0 + c;
 #pragma unroll
-                    for (int j = 0; j < 16; j++)
-                        atomicAdd(d + j, v[j]);
+                        for (int j = 0; j < 16; j++)
+                            atomicAdd(d + j, v[j]);
+                    }
                 }
             }
         }
