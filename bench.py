@@ -408,9 +408,11 @@ def run_ours(args):
                 "roofline": roof, "e2e": e2e,
                 # per time step one fused launch forward and one reverse (the
                 # unfused variant 4: a P and an A launch in each); per
-                # gradient the misfit, its sum, the running integral, shot mean
+                # gradient the misfit, its sum, the running integral, shot
+                # mean, and for variants 4 and 5 one check kernel after each
+                # time loop (launch count, tickets)
                 "gpu_launches": args.steps * ((4 if args.kernel == 4 else 2) * (sc.T - 1) + 4
-                                              + (2 if args.kernel == 5 else 0)),
+                                              + (2 if args.kernel in (4, 5) else 0)),
                 "clocks": clk.summary(),
                 "misfit_value": float(mis.item())}
         if not args.no_cpu_baseline and world == 1:
