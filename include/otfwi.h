@@ -152,6 +152,11 @@ int otf_batch_set_paired_lead(otf_batch *b, int lead);
 /* Row-lag fused kernels (variant 6): rows per chunk of a CTA (default 64,
  * >= 8; each chunk recomputes P(t) on 4 rows above and below it). */
 int otf_batch_set_fused_rows(otf_batch *b, int rows);
+/* Unfused kernels (variant 4): the shots split into `lanes` groups whose time
+ * loops run as parallel launch chains inside the captured graph (0, the
+ * default: one per 16 shots, at most 4; 1: one chain; OTFWI_LANES sets the
+ * default). Results are bit-identical for every setting. */
+int otf_batch_set_lanes(otf_batch *b, int lanes);
 /* Forward modelling of every shot; traces [n_shots][n_rec][T] (NULL: keep). */
 int otf_batch_forward(otf_batch *b, float *traces, int on_device);
 /* Forward with boundary-ring recording (gradient phase 1). */
@@ -211,6 +216,9 @@ int otf_batch_last_gradient(otf_batch *b, float *grad, double *misfit, int on_de
 typedef struct otf_multi otf_multi;
 otf_multi *otf_multi_create(int n, otf_batch **batches);
 void otf_multi_destroy(otf_multi *m);
+/* chains > 0: instance i starts after instance i - chains has finished, so
+ * at most `chains` instances run at once (0, the default: all at once). */
+int otf_multi_set_chains(otf_multi *m, int chains);
 int otf_multi_gradient(otf_multi *m, int misfit_kind);
 int otf_multi_sync(otf_multi *m);
 

@@ -41,6 +41,7 @@ def _declare(lib):
         "otf_batch_set_stream_rows": [c_void_p, c_int],
         "otf_batch_set_paired_lead": [c_void_p, c_int],
         "otf_batch_set_fused_rows": [c_void_p, c_int],
+        "otf_batch_set_lanes": [c_void_p, c_int],
         "otf_batch_forward": [c_void_p, c_void_p, c_int],
         "otf_batch_forward_ring": [c_void_p, c_void_p, c_int],
         "otf_batch_gradient": [c_void_p, c_int, c_void_p, c_void_p, c_int],
@@ -193,6 +194,11 @@ class ShotBatch:
         step (fast numerics); 6: row-lag fused half-steps, one pass per step
         (fast numerics)."""
         self._ok(self._lib.otf_batch_set_kernel(self._h, variant))
+
+    def set_lanes(self, lanes):
+        """Shot groups run as parallel launch chains by the unfused kernels
+        (0: automatic, one per 16 shots up to 4; 1: one chain)."""
+        self._ok(self._lib.otf_batch_set_lanes(self._h, int(lanes)))
 
     def set_fused_rows(self, rows):
         """Rows per chunk of the row-lag fused kernels (variant 6, >= 8)."""

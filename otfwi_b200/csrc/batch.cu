@@ -68,6 +68,13 @@ int otf_batch_set_precision(otf_batch *b, int precision) { return b->eng.set_pre
 int otf_batch_set_tile(otf_batch *b, int tile) { return b->eng.set_tile(tile); }
 int otf_batch_set_kernel(otf_batch *b, int variant) { return b->eng.set_variant(variant); }
 int otf_batch_set_stream_rows(otf_batch *b, int rows) { return b->eng.set_stream_rows(rows); }
+int otf_batch_set_lanes(otf_batch *b, int lanes)
+{
+    OTF_CHECK(b && lanes >= 0, 1, "otf_batch_set_lanes: bad arguments");
+    b->eng.set_lanes(lanes);
+    return 0;
+}
+
 int otf_batch_set_fused_rows(otf_batch *b, int rows)
 {
     OTF_CHECK(rows >= 8, 1, "fused rows per chunk must be >= 8");
@@ -259,6 +266,7 @@ int otf_batch_last_gradient(otf_batch *b, float *grad, double *misfit, int on_de
 // so one launch runs them all and the GPU fills its SMs from every branch.
 struct otf_multi {
     std::vector<otf_batch *> b;
+    int chains = 0;  // > 0: instance i runs after instance i - chains (that many branches at once)
     cudaStream_t st = nullptr;
     cudaGraphExec_t exec[otf::kNumMisfits] = {};
     ~otf_multi()
@@ -291,12 +299,26 @@ otf_multi *otf_multi_create(int n, otf_batch **batches)
 
 void otf_multi_destroy(otf_multi *m) { delete m; }
 
+int otf_multi_set_chains(otf_multi *m, int chains)
+{
+    OTF_CHECK(m && chains >= 0, 1, "otf_multi_set_chains: bad arguments");
+    if (chains != m->chains)
+        for (auto &e : m->exec)
+            if (e) {
+                cudaGraphExecDestroy(e);
+                e = nullptr;
+            }
+    m->chains = chains;
+    return 0;
+}
+
 int otf_multi_gradient(otf_multi *m, int misfit_kind)
 {
     OTF_CHECK(misfit_kind >= 0 && misfit_kind < otf::kNumMisfits, 1, "unknown misfit kind");
     if (!m->exec[misfit_kind]) {
         cudaGraph_t parent = nullptr;
         OTF_CUDA(cudaGraphCreate(&parent, 0));
+        std::vector<cudaGraphNode_t> nodes;
         for (otf_batch *b : m->b) {
             cudaGraph_t child = nullptr;
             if (b->eng.gradient_graph(misfit_kind, &child)) {
@@ -304,7 +326,11 @@ int otf_multi_gradient(otf_multi *m, int misfit_kind)
                 return -1;
             }
             cudaGraphNode_t node;
-            const cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
+            const size_t i = nodes.size();
+            const bool dep = m->chains > 0 && i >= (size_t)m->chains;
+            const cudaError_t e =
+                cudaGraphAddChildGraphNode(&node, parent, dep ? &nodes[i - m->chains] : nullptr, dep ? 1 : 0, child);
+            nodes.push_back(node);
             cudaGraphDestroy(child);
             if (e != cudaSuccess) {
                 cudaGraphDestroy(parent);

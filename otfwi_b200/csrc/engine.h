@@ -121,6 +121,9 @@ class Engine {
     void set_paired_lead(int lead) { pair_lead_ = lead; drop_graphs(); }
     // fused kernels: rows per chunk (>= 8)
     void set_fused_rows(int rows) { fused_rows_ = rows < 8 ? 8 : rows; drop_graphs(); }
+    // shot groups run as parallel launch chains by the unfused kernels (0:
+    // automatic, one per 16 shots up to kMaxLanes; 1: one chain)
+    void set_lanes(int lanes) { lanes_req_ = lanes < 0 ? 0 : lanes; drop_graphs(); }
     // rows per segment of the z-streaming kernels (>= 8)
     int set_stream_rows(int rows);
     int variant_in_use() const;
@@ -148,7 +151,10 @@ class Engine {
     UnfusedParams unfused_params(const StepParams &p, int kind) const;
     int paired_lead(int kind) const;
     int begin_steps();             // before a time loop of step launches
-    int end_steps(int n_steps);    // after it
+    int end_steps(int n_steps, int lanes = 1);  // after it
+    int lanes_in_use() const;      // shot groups of the unfused time loops
+    template <class Step>
+    int lane_loop(int lanes, Step step);  // step(t) for every lane's shots, lanes as parallel chains
     void drop_graphs();
     StepParams base_params() const;
     void free_all();
@@ -163,6 +169,16 @@ class Engine {
     std::vector<int> shot_ptr_, shot_srcs_;
 
     cudaStream_t st_ = nullptr;
+    // lanes: the unfused time loops split the shots into up to kMaxLanes
+    // groups, each its own chain of launches (lane 0 on st_), forked from and
+    // joined back into st_ inside the captured graph
+    static constexpr int kMaxLanes = 4;
+    cudaStream_t lane_st_[kMaxLanes] = {};
+    cudaEvent_t lane_ev_[kMaxLanes] = {};
+    int lanes_req_ = 0;  // 0: automatic
+    // launch context of the unfused kernels inside a time loop (0: every shot on st_)
+    cudaStream_t ust_ = nullptr;
+    int ushot0_ = 0, ushots_ = 0;
     // device buffers
     float *qf_ = nullptr, *qr_ = nullptr;                            // padded P coefficients
     float *cq_stage_ = nullptr;                                      // [Z*X] staging of a host model

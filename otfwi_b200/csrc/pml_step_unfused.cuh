@@ -72,6 +72,7 @@ struct UnfusedParams {
     const int *rec_off, *ring_off;
     int record_ring;  // forward: also record the boundary ring
     unsigned *ledger;  // launches of this time loop: the first CTA of each launch counts it
+    int shot0;         // first shot of this launch (a lane of the batch: grid z covers its shots)
 };
 
 // Count this launch (thread 0 of the first CTA), after pdl_enter: a launch
@@ -243,8 +244,8 @@ __device__ __forceinline__ void cta_inject(const StepParams &p, const Fields &f,
 constexpr int kUPMinBlocks = 24;
 constexpr int kUAMinBlocks = 28;
 
-// Forward P half-step and the sources: grid (ncb, nseg, n_shots), shots
-// upwards.
+// Forward P half-step and the sources: grid (ncb, nseg, shots of the
+// launch), shots upwards.
 __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
@@ -252,9 +253,9 @@ __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     const int cta = blockIdx.x + U.ncb * blockIdx.y;
     if (x < U.p.X)
-        p_segment<false>(U, U.p.f0, U.p.q0, blockIdx.z, x, blockIdx.y * kURows);
+        p_segment<false>(U, U.p.f0, U.p.q0, U.shot0 + (int)blockIdx.z, x, blockIdx.y * kURows);
     __syncwarp();
-    cta_inject(U.p, U.p.f0, blockIdx.z, U.src_cta, U.src_off, U.src_ptr, U.src_id, cta, true);
+    cta_inject(U.p, U.p.f0, U.shot0 + (int)blockIdx.z, U.src_cta, U.src_off, U.src_ptr, U.src_id, cta, true);
 }
 
 // Reverse P half-steps of both sets: grid (ncb, nseg, 2 * n_shots), shot
@@ -268,7 +269,7 @@ __global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_rev(const
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     const int cta = blockIdx.x + U.ncb * blockIdx.y;
     const bool rec_set = (blockIdx.z & 1u) == 0u;
-    const int shot = (int)(blockIdx.z >> 1);
+    const int shot = U.shot0 + (int)(blockIdx.z >> 1);
     if (x < p.X) {
         if (rec_set)
             p_segment<true>(U, p.f0, p.q0, shot, x, blockIdx.y * kURows);
@@ -378,7 +379,7 @@ __global__ void __launch_bounds__(kUThreads, kUAMinBlocks) k_unfused_a_fwd(const
     pdl_enter();
     count_launch(U);
     const StepParams &p = U.p;
-    const int shot = (int)(gridDim.z - 1u - blockIdx.z);
+    const int shot = U.shot0 + (int)(gridDim.z - 1u - blockIdx.z);
     const int64_t so = p.shot_stride * shot;
     const float *__restrict__ P = p.f0.px_out + so;
     const int n_tail = gridDim.y - U.nseg;
@@ -647,7 +648,7 @@ __global__ void __launch_bounds__(kUThreads, MINB) k_unfused_a_rev_sets(const __
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= U.p.X)
         return;
-    const int shot = (int)(gridDim.z / 2u - 1u - (blockIdx.z >> 1));
+    const int shot = U.shot0 + (int)(gridDim.z / 2u - 1u - (blockIdx.z >> 1));
     if ((blockIdx.z & 1u) == 0u)
         a_rev_rec_segment(U, shot, x, blockIdx.y * kURows);
     else
@@ -663,7 +664,7 @@ __global__ void __launch_bounds__(kUThreads) k_unfused_a_rev(const __grid_consta
     const int x = blockIdx.x * kUCols + 4 * threadIdx.x;
     if (x >= U.p.X)
         return;
-    a_rev_segment<false>(U, (int)(gridDim.z - 1u - blockIdx.z), x, blockIdx.y * kURows);
+    a_rev_segment<false>(U, U.shot0 + (int)(gridDim.z - 1u - blockIdx.z), x, blockIdx.y * kURows);
 }
 
 }  // namespace otf
