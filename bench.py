@@ -256,6 +256,7 @@ def run_ours(args):
     b = ShotBatch(sc.X, sc.Z, sc.T, sc.PML, sc.src_mask, sc.rec_mask, sc.source, prec_deriv=4,
                   precision=args.precision, tile=args.tile, kernel=args.kernel, shots=shots)
     b.set_stream_rows(args.stream_rows)
+    lanes = b.lanes()
     dev = torch.device("cuda", local)
     stream = torch.cuda.ExternalStream(b.stream(), device=dev)
     c_true = torch.tensor(sc.c_true, dtype=torch.float32, device=dev)
@@ -407,11 +408,11 @@ def run_ours(args):
                            "stream_rows": args.stream_rows if args.kernel == 3 else None},
                 "roofline": roof, "e2e": e2e,
                 # per time step one fused launch forward and one reverse (the
-                # unfused variant 4: a P and an A launch in each); per
-                # gradient the misfit, its sum, the running integral, shot
-                # mean, and for variants 4 and 5 one check kernel after each
-                # time loop (launch count, tickets)
-                "gpu_launches": args.steps * ((4 if args.kernel == 4 else 2) * (sc.T - 1) + 4
+                # unfused variant 4: a P and an A launch in each, per shot
+                # lane); per gradient the misfit, its sum, the running
+                # integral, shot mean, and for variants 4 and 5 one check
+                # kernel after each time loop (launch count, tickets)
+                "gpu_launches": args.steps * ((4 * lanes if args.kernel == 4 else 2) * (sc.T - 1) + 4
                                               + (2 if args.kernel in (4, 5) else 0)),
                 "clocks": clk.summary(),
                 "misfit_value": float(mis.item())}

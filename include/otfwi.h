@@ -157,6 +157,9 @@ int otf_batch_set_fused_rows(otf_batch *b, int rows);
  * default: one per 16 shots, at most 4; 1: one chain; OTFWI_LANES sets the
  * default). Results are bit-identical for every setting. */
 int otf_batch_set_lanes(otf_batch *b, int lanes);
+/* The lanes the batch's time loops use with its current settings (1 for
+ * every variant but the unfused kernels). */
+int otf_batch_lanes(otf_batch *b);
 /* Forward modelling of every shot; traces [n_shots][n_rec][T] (NULL: keep). */
 int otf_batch_forward(otf_batch *b, float *traces, int on_device);
 /* Forward with boundary-ring recording (gradient phase 1). */

@@ -42,6 +42,7 @@ def _declare(lib):
         "otf_batch_set_paired_lead": [c_void_p, c_int],
         "otf_batch_set_fused_rows": [c_void_p, c_int],
         "otf_batch_set_lanes": [c_void_p, c_int],
+        "otf_batch_lanes": [c_void_p],
         "otf_batch_forward": [c_void_p, c_void_p, c_int],
         "otf_batch_forward_ring": [c_void_p, c_void_p, c_int],
         "otf_batch_gradient": [c_void_p, c_int, c_void_p, c_void_p, c_int],
@@ -199,6 +200,10 @@ class ShotBatch:
         """Shot groups run as parallel launch chains by the unfused kernels
         (0: automatic, one per 16 shots up to 4; 1: one chain)."""
         self._ok(self._lib.otf_batch_set_lanes(self._h, int(lanes)))
+
+    def lanes(self):
+        """Lanes (parallel launch chains) of this batch's time loops."""
+        return int(self._lib.otf_batch_lanes(self._h))
 
     def set_fused_rows(self, rows):
         """Rows per chunk of the row-lag fused kernels (variant 6, >= 8)."""

@@ -75,6 +75,8 @@ int otf_batch_set_lanes(otf_batch *b, int lanes)
     return 0;
 }
 
+int otf_batch_lanes(otf_batch *b) { return b ? b->eng.lanes_in_use() : -1; }
+
 int otf_batch_set_fused_rows(otf_batch *b, int rows)
 {
     OTF_CHECK(rows >= 8, 1, "fused rows per chunk must be >= 8");

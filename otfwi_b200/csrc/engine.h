@@ -124,6 +124,7 @@ class Engine {
     // shot groups run as parallel launch chains by the unfused kernels (0:
     // automatic, one per 16 shots up to kMaxLanes; 1: one chain)
     void set_lanes(int lanes) { lanes_req_ = lanes < 0 ? 0 : lanes; drop_graphs(); }
+    int lanes_in_use() const;  // lanes of the time loops with the current settings
     // rows per segment of the z-streaming kernels (>= 8)
     int set_stream_rows(int rows);
     int variant_in_use() const;
@@ -152,7 +153,6 @@ class Engine {
     int paired_lead(int kind) const;
     int begin_steps();             // before a time loop of step launches
     int end_steps(int n_steps, int lanes = 1);  // after it
-    int lanes_in_use() const;      // shot groups of the unfused time loops
     template <class Step>
     int lane_loop(int lanes, Step step);  // step(t) for every lane's shots, lanes as parallel chains
     void drop_graphs();
