@@ -1,6 +1,7 @@
 """GPU tests of the uneven multi-instance group: independent inversions of
 different grid sizes, shot counts and T computed as parallel branches of one
-CUDA graph must give exactly their stand-alone gradients, and each small
+CUDA graph (or as chains of branches, otf_multi_set_chains) must give
+exactly their stand-alone gradients, and each small
 instance's gradient is checked against the FP64 oracle (relative L2 <= 1e-3,
 fast numerics)."""
 import numpy as np
@@ -42,6 +43,16 @@ def test_multi_instance_graph_equals_standalone(lib):
     again = m.gradient("wasserstein")
     for (g0, _), (g1, _) in zip(together, again):
         assert np.array_equal(g0, g1)
+    # the instances as chains (one at a time, then two at once): the same
+    import ctypes
+    L = m._lib
+    L.otf_multi_set_chains.restype = ctypes.c_int
+    L.otf_multi_set_chains.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    for chains in (1, 2):
+        assert L.otf_multi_set_chains(m._h, chains) == 0
+        chained = m.gradient("wasserstein")
+        for (g0, m0), (g1, m1) in zip(alone, chained):
+            assert np.array_equal(g0, g1) and m0 == m1, chains
 
 
 def test_multi_instance_gradients_vs_fp64_oracle(lib):
