@@ -669,9 +669,8 @@ int conv_umma_launch(const ConvArgs &a, const ConvMaps &maps, int nb, int nk, in
         const int ncb = cout / nb;
         int gx = sms * cps / ncb;
         gx = gx < 1 ? 1 : (gx > tiles ? tiles : gx);
-        auto kern = k_conv3x3_umma_pers<true, kResStages>;
-        OTF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        kern<<<dim3((unsigned)gx, (unsigned)ncb), 256, smem, st>>>(a, maps, nb, tiles);
+        OTF_CUDA(cudaFuncSetAttribute(k_conv3x3_umma_res, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        k_conv3x3_umma_res<<<dim3((unsigned)gx, (unsigned)ncb), 256, smem, st>>>(a, maps, nb, tiles);
         return launch_status();
     }
     const dim3 grid((unsigned)tiles, (unsigned)(cout / nb));

@@ -408,39 +408,38 @@ __global__ void __launch_bounds__(128) k_conv3x3_umma(const __grid_constant__ Co
     }
 }
 
-// Persistent forms for the layers with at most 128 output channels per CTA:
-// the CTA walks 256-pixel tiles blockIdx.x, + gridDim.x, ...; two
-// accumulator buffers (2 x 2N tensor-memory columns) let the epilogue of one
-// tile overlap the MMAs of the next. RES (the small layers, all of the CTA's
-// weights within kResWeightBytes): the weights of every chunk and tap stay in
-// shared memory for the CTA's life (one TMA load per chunk and plane at the
-// start, then only halo tiles stream). Otherwise each stage carries a chunk's
-// halo and its weights, NST stages deep. Warps: 0 producer (TMA loads; with
-// warps 6 and 7 the cp.async gather of an upsampled chunk), 1 the MMA
-// issuer (one thread), 2-5 the epilogue (TMEM lane quarters 2, 3, 0, 1). Per
-// stage a full (three producer warps) / empty (MMA commit) barrier pair; per
-// accumulator buffer a full (MMA commit) / empty (four epilogue warps) pair.
-// Bounded waits as the kernel above; a failed wait sets the error flag, the
-// role stops, and teardown waits (bounded) for the MMAs and copies issued.
+// Persistent form for the small layers (at most 128 output channels per CTA
+// and all of the CTA's weights within kResWeightBytes): the weights of every
+// chunk and tap stay in shared memory for the CTA's life (loaded once at the
+// start; then only halo tiles stream); the CTA walks 256-pixel tiles
+// blockIdx.x, + gridDim.x, ...; two accumulator buffers (2 x 2N
+// tensor-memory columns) let the epilogue of one tile overlap the MMAs of the
+// next. (With the weights streamed with the halo instead, the persistent form
+// measured slower than one tile per CTA on the large layers.) Warps: 0
+// producer (TMA loads; with warps 6 and 7 the cp.async gather of an
+// upsampled chunk), 1 the MMA issuer (one thread), 2-5 the epilogue (TMEM
+// lane quarters 2, 3, 0, 1). Per halo stage a full (three producer warps) /
+// empty (MMA commit) barrier pair; per accumulator buffer a full (MMA commit)
+// / empty (four epilogue warps) pair. Bounded waits as the kernel above; a
+// failed wait sets the error flag, the role stops, and teardown waits
+// (bounded) for the MMAs and copies issued.
 constexpr int kResWeightBytes = 96 * 1024;
 constexpr int kResStages = 4;
 __host__ __device__ constexpr int umma_res_smem_bytes(int n, int nk)
 {
     return nk * 2 * 9 * n * 16 + kResStages * 2 * umma::PLANE2 + 256;
 }
-// streamed weights: NST stages of (two halo planes, two weight planes)
-__host__ __device__ constexpr int umma_pers_smem_bytes(int n, int nst) { return nst * umma_stage_bytes(n) + 256; }
 
-template <bool RES, int NST>
-__global__ void __launch_bounds__(256) k_conv3x3_umma_pers(const __grid_constant__ ConvArgs a,
-                                                          const __grid_constant__ ConvMaps maps, int N, int n_tiles)
+__global__ void __launch_bounds__(256) k_conv3x3_umma_res(const __grid_constant__ ConvArgs a,
+                                                         const __grid_constant__ ConvMaps maps, int N, int n_tiles)
 {
     extern __shared__ __align__(1024) unsigned char smu[];
+    constexpr int NST = kResStages;
     const int cin = a.c0 + a.c1, nk = cin / KC;
     const int wchunk = 2 * 9 * N * 16;          // bytes of one chunk's weights (two planes)
-    unsigned char *wsm = smu;                   // RES: [chunk][plane][tap][co][8 ch]
-    unsigned char *hsm = RES ? smu + nk * wchunk : smu;  // NST stages
-    const int SA = 2 * umma::PLANE2 + (RES ? 0 : wchunk);  // a stage: halo planes (+ chunk weights)
+    unsigned char *wsm = smu;                   // [chunk][plane][tap][co][8 ch]
+    unsigned char *hsm = smu + nk * wchunk;     // NST halo stages
+    constexpr int SA = 2 * umma::PLANE2;        // a stage: two halo planes
     uint64_t *full = reinterpret_cast<uint64_t *>(hsm + NST * SA);
     uint64_t *empty = full + NST;
     uint64_t *acc_full = empty + NST;
@@ -496,13 +495,9 @@ __global__ void __launch_bounds__(256) k_conv3x3_umma_pers(const __grid_constant
             otf::tma_prefetch_desc(&maps.x0);
             if (a.c1 && !a.up1)
                 otf::tma_prefetch_desc(&maps.x1);
-            if (RES) {
-                otf::mbar_arrive_expect_tx(wbar, (uint32_t)(nk * wchunk));
-                for (int kc = 0; kc < nk; kc++)
-                    load_chunk_weights(wsm + kc * wchunk, a, maps, kc, co0, N, wbar);
-            } else {
-                otf::mbar_arrive(wbar);  // nothing resident to wait for
-            }
+            otf::mbar_arrive_expect_tx(wbar, (uint32_t)(nk * wchunk));
+            for (int kc = 0; kc < nk; kc++)
+                load_chunk_weights(wsm + kc * wchunk, a, maps, kc, co0, N, wbar);
         }
         const uint32_t abytes = 2u * umma::HPIX2 * 16u;
         int g = 0;
@@ -527,16 +522,12 @@ __global__ void __launch_bounds__(256) k_conv3x3_umma_pers(const __grid_constant
                 const int ch = kc * KC;
                 const bool from1 = ch >= a.c0;
                 const bool gather = from1 && a.up1;
-                if (warp == 0 && lane == 0 && (!gather || !RES)) {
-                    otf::mbar_expect_tx(&full[s], (gather ? 0u : abytes) + (RES ? 0u : (uint32_t)wchunk));
-                    if (!RES)
-                        load_chunk_weights(st + 2 * umma::PLANE2, a, maps, kc, co0, N, &full[s]);
-                    if (!gather) {
-                        const CUtensorMap *mx = from1 ? &maps.x1 : &maps.x0;
-                        const int c = from1 ? ch - a.c0 : ch;
-                        for (int h = 0; h < 2; h++)
-                            otf::tma_load_4d(st + h * umma::PLANE2, mx, c + 8 * h, x0 - 1, y0 - 1, n, &full[s]);
-                    }
+                if (warp == 0 && lane == 0 && !gather) {
+                    otf::mbar_expect_tx(&full[s], abytes);
+                    const CUtensorMap *mx = from1 ? &maps.x1 : &maps.x0;
+                    const int c = from1 ? ch - a.c0 : ch;
+                    for (int h = 0; h < 2; h++)
+                        otf::tma_load_4d(st + h * umma::PLANE2, mx, c + 8 * h, x0 - 1, y0 - 1, n, &full[s]);
                 }
                 if (gather)
                     conv_gather(a, st, ch, n, y0, x0, pi, 3, lane);
@@ -573,7 +564,7 @@ __global__ void __launch_bounds__(256) k_conv3x3_umma_pers(const __grid_constant
                     }
                     umma::fence_after_sync();
                     const uint32_t abase = otf::smem_u32(hsm + s * SA);
-                    const uint32_t bbase = RES ? otf::smem_u32(wsm + kc * wchunk) : abase + 2 * umma::PLANE2;
+                    const uint32_t bbase = otf::smem_u32(wsm + kc * wchunk);
 #pragma unroll
                     for (int tap = 0; tap < 9; tap++) {
                         const int dy = tap / 3, dx = tap - 3 * (tap / 3);
