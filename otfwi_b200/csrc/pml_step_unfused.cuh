@@ -239,16 +239,17 @@ __device__ __forceinline__ void cta_inject(const StepParams &p, const Fields &f,
 }
 
 // Resident CTAs each kernel is compiled for (a register cap), from
-// measurements: 24 (80 registers) for the P kernels, 28 (72) for the forward
-// A kernel; the reverse A kernel needs its 128 registers. The row loops of
+// measurements: 24 (80 registers) for the reverse P kernel, 28 (72) for the
+// forward P and A kernels, 20 (96) for the reverse A kernel. The row loops of
 // the P half-step and of the reverse adjoint A half-step are not unrolled
 // (measured 2-3% faster than unrolled by 2 on the reverse step).
 constexpr int kUPMinBlocks = 24;
+constexpr int kUPFwdMinBlocks = 28;  // the forward P kernel fits 72 registers without spilling
 constexpr int kUAMinBlocks = 28;
 
 // Forward P half-step and the sources: grid (ncb, nseg, shots of the
 // launch), shots upwards.
-__global__ void __launch_bounds__(kUThreads, kUPMinBlocks) k_unfused_p_fwd(const __grid_constant__ UnfusedParams U)
+__global__ void __launch_bounds__(kUThreads, kUPFwdMinBlocks) k_unfused_p_fwd(const __grid_constant__ UnfusedParams U)
 {
     pdl_enter();
     count_launch(U);
