@@ -15,17 +15,24 @@
 //                            reverted; then P_rec(t) = ring(T-1-t) on the
 //                            CTA's ring cells) and adjoint (damped; then the
 //                            adjoint sources at the CTA's receivers)
-//                  A kernel  both A updates, the 9-point Laplacian of
-//                            P_rec(t) and grad += P_adj(t) * lap
+//                  A kernel  one CTA per field set: the reconstruction's A
+//                            update, the 9-point Laplacian of P_rec(t) and
+//                            grad += P_adj(t) * lap; the adjoint's damped A
+//                            update (k_unfused_a_rev_sets; both sets in one
+//                            CTA: k_unfused_a_rev)
+//
+// Within a time loop the engine may split the shots into lanes, each its own
+// chain of these launches (grid z = the lane's shots, UnfusedParams::shot0
+// its first): the lanes run concurrently and fill each other's launch tails.
 //
 // A thread owns 4 adjacent columns (16-byte loads and stores) of a
 // 128-column block and marches down kURows rows: z-derivatives come from a
 // sliding register window per column, x-derivatives from three 16-byte row
 // loads (columns x-4 .. x+7) that L1 shares between neighbouring threads.
 // One warp per CTA, no shared memory, no barrier. Bytes per cell: 40 for a
-// forward step (P kernel 20 + Q on damped cells, A kernel 20), 88 for a
-// reverse step, against 28 and 64 for the fused kernels, at 80-90% of the
-// bandwidth instead of under 50%.
+// forward step (P kernel 20 + Q on damped cells, A kernel 20), 92 for a
+// reverse step (P 40, A 52), against 28 and 64 for the fused kernels, at
+// 70-80% of the bandwidth instead of under 50%.
 //
 // Shot order alternates between consecutive launches: CTAs are dispatched in
 // grid order, the P kernels walk the shots upwards and the A kernels
